@@ -1,0 +1,88 @@
+"""CPU-only checks: the C-ABI library loads and exports every declared symbol,
+and its host-side arithmetic (header decode, MJD, layout, delay table)
+matches the oracle exactly."""
+import ctypes
+import os
+import re
+
+import numpy as np
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def _declared_functions():
+    txt = open(os.path.join(ROOT, "include", "vfrb.h")).read()
+    txt = re.sub(r"/\*.*?\*/", "", txt, flags=re.S)
+    return sorted(set(re.findall(r"\b(vfrb_\w+)\s*\(", txt)))
+
+
+def test_library_exports_every_declared_symbol(vf):
+    names = _declared_functions()
+    assert len(names) >= 14
+    lib = ctypes.CDLL(vf.LIB_PATH)
+    missing = [n for n in names if not hasattr(lib, n)]
+    assert not missing, missing
+
+
+def test_header_decode_matches_oracle(vf, O):
+    rng = np.random.default_rng(0)
+    for _ in range(200):
+        b = rng.integers(0, 256, 32, dtype=np.uint8).tobytes()
+        a = vf.decode_header(b)
+        o = O.decode_header(b)
+        assert a["seconds"] == o["seconds"] and a["frame"] == o["frame"] and a["epoch"] == o["epoch"]
+        assert a["threadid"] == o["threadid"] and a["invalid"] == o["invalid"] and a["legacymode"] == o["legacymode"]
+        assert a["framelength8"] == o["framelength8"] and a["nbits_minus1"] == o["nbits"]
+        assert a["stationid"] == o["stationid"] and a["iscomplex"] == o["iscomplex"]
+        assert a["extended1"] == o["extended1"] and a["extended4"] == o["extended4"]
+        assert vf.header_dmjd(b) == O.vdif_dmjd(o)
+
+
+def test_header_roundtrip_known_values(vf, O):
+    b = O.encode_header(seconds=12345678, frame=25599, epoch=33, framelength8=629, threadid=1, nbits=7,
+                        stationid=0x5858, invalid=1)
+    h = vf.decode_header(b)
+    assert (h["seconds"], h["frame"], h["epoch"], h["threadid"], h["invalid"]) == (12345678, 25599, 33, 1, 1)
+    # epoch 33 = 2016-07-01 (MJD 57570); 12345678 s = 142 d + 76878 s
+    assert abs(vf.header_dmjd(b) - (57570 + 142 + 76878 / 86400 + 25599 / (25600 * 86400))) < 1e-9
+
+
+@pytest.mark.parametrize("twonchan,nave,nb,muos,fixed,maxtime", [
+    (12500, 4, 32, 360.0, 0, 70.0), (12500, 10, 32, 384.0, 0, 60.0), (12500, 4, 32, 360.0, 3840, 30.0),
+    (12500, 4, 32, 360.0, 0, 60.0), (8000, 3, 16, 360.0, 0, 7.5), (12500, 10, 32, 384.0, 0, 7.5)])
+def test_layout_matches_oracle(vf, O, twonchan, nave, nb, muos, fixed, maxtime):
+    L = vf.layout(twonchan, nave, nb, muos, fixed, maxtime)
+    o = O.Layout(twonchan=twonchan, nave=nave, nbundle=nb, muoslowfreq=muos, maxtime=maxtime,
+                 nchanout_fixed=fixed or None)
+    for k in ("nchan", "nfreq", "nchanout", "nskip", "nloop", "maxnt", "nhalfcyc"):
+        assert getattr(L, k) == getattr(o, k), k
+    for k in ("chanbw", "fch1", "foff", "tchan"):
+        assert getattr(L, k) == getattr(o, k), k
+
+
+def test_layout_reference_values(vf):
+    L = vf.layout(12500, 10, 32, 384.0, 0, 60.0)
+    assert (L.nchanout, L.nskip, L.maxnt) == (6250, 1, 61440)
+    assert abs(L.fch1 - 383.99488) < 1e-9 and abs(L.tchan - 0.0009765625) < 1e-15
+    L = vf.layout(12500, 4, 32, 360.0, 0, 70.0)
+    assert (L.nchanout, L.nskip, L.maxnt, L.nhalfcyc) == (3908, 2343, 179200, 1400)
+
+
+def test_delay_table_matches_oracle(vf, O):
+    L = vf.layout(12500, 10, 32, 384.0, 0, 60.0)
+    dms = np.linspace(0, 1000, 2048).astype(np.float32)[::97]
+    off, md = vf.delay_table(L, dms)
+    o_off, o_md = O.delay_table(dms, L.fch1, L.chanbw, L.tchan, L.nchanout)
+    assert np.array_equal(off, o_off) and md == o_md
+    # TS: DM {0, 119.3}, 3840 channels (TS:441-464)
+    L = vf.layout(12500, 4, 32, 360.0, 3840, 30.0)
+    off, md = vf.delay_table(L, np.array([0.0, 119.3], np.float32))
+    o_off, o_md = O.delay_table(np.array([0.0, 119.3], np.float32), L.fch1, L.chanbw, L.tchan, L.nchanout)
+    assert np.array_equal(off, o_off) and md == o_md and off[0].max() == 0
+
+
+def test_dm1000_sweep(vf):
+    L = vf.layout(12500, 10, 32, 384.0, 0, 60.0)
+    off, md = vf.delay_table(L, np.array([1000.0], np.float32))
+    assert 12600 < md < 12700 and off.max() <= md

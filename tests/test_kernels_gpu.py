@@ -1,0 +1,284 @@
+"""Stage-level parity of the sm_100a kernels against the FP64 oracle.
+
+Tolerances (stated here, used below):
+  * channeliser FB (FP32) vs FP64: max per-element relative error <= 1e-5;
+  * bandpass output: |gpu - oracle| <= 1e-6 * max|input| (one float rounding);
+  * dedispersed series (FP32): max |gpu - oracle| <= 1e-5 * rms(oracle series);
+  * per-DM ave/sigma: relative <= 1e-5; peak: relative <= 1e-4; FRB flag exact;
+  * FP16 storage: <= 3e-3 * rms, int8 (q=16) storage: <= 0.12 * rms (errors reported);
+  * per-channel stats: relative <= 1e-6, outlier fraction exact.
+"""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def _torch():
+    import torch
+    return torch
+
+
+def _frames(duration, seed=0, pulses=()):
+    from vlite_frb_b200 import synth
+    return synth.make_vdif(synth.StreamSpec(duration=duration, seed=seed, pulses=list(pulses)))
+
+
+def _pol_streams(buf_np):
+    fr = buf_np.reshape(-1, 2, 5032)
+    return fr[:, 0, 32:].reshape(-1), fr[:, 1, 32:].reshape(-1)
+
+
+@pytest.mark.parametrize("muos,nave,fixed", [(384.0, 10, 0), (360.0, 4, 0), (360.0, 10, 3840)])
+def test_channelise_matches_fp64(vf, O, muos, nave, fixed):
+    torch = _torch()
+    buf = _frames(0.15, seed=3)
+    L = vf.layout(nave=nave, muoslowfreq=muos, nchanout_fixed=fixed)
+    Lo = O.Layout(nave=nave, muoslowfreq=muos, nchanout_fixed=(fixed or None))
+    assert (L.nchanout, L.nskip) == (Lo.nchanout, Lo.nskip)
+    p0, p1 = _pol_streams(buf.numpy())
+    nrows = len(p0) // (nave * 12500)
+    ref = O.channelise(p0, p1, Lo)[:nrows]
+    dev = torch.device("cuda")
+    d = buf.to(dev)
+    npairs = buf.numel() // (2 * 5032)
+    idx = torch.arange(npairs, dtype=torch.int64, device=dev)
+    s0 = idx * (2 * 5032) + 32
+    s1 = s0 + 5032
+    err = torch.zeros(1, dtype=torch.int32, device=dev)
+    fb = vf.channelise(d, s0, s1, 0, nrows, L, d_err=err)
+    torch.cuda.synchronize()
+    assert int(err.item()) == 0
+    got = fb.cpu().numpy().astype(np.float64)
+    rel = np.abs(got - ref) / np.abs(ref)
+    print("channelise max rel err", rel.max(), "nchanout", L.nchanout)
+    assert rel.max() <= 1e-5
+
+
+def test_channelise_unaligned_and_ring(vf, O):
+    """sample0 not a multiple of 4 (byte path) and output into a wrapped ring."""
+    torch = _torch()
+    buf = _frames(0.05, seed=5)
+    L = vf.layout(nave=2, muoslowfreq=384.0)
+    Lo = O.Layout(nave=2, muoslowfreq=384.0)
+    p0, p1 = _pol_streams(buf.numpy())
+    off = 3
+    nrows = (len(p0) - off) // (2 * 12500)
+    ref = O.channelise(p0[off:], p1[off:], Lo)[:nrows]
+    dev = torch.device("cuda")
+    d = buf.to(dev)
+    npairs = buf.numel() // (2 * 5032)
+    idx = torch.arange(npairs, dtype=torch.int64, device=dev)
+    s0 = idx * (2 * 5032) + 32
+    ring = torch.full((64, L.nchanout), -1.0, device=dev)
+    fb = vf.channelise(d, s0, s0 + 5032, off, nrows, L, out=ring, out_row0=50, out_row_mask=63)
+    torch.cuda.synchronize()
+    got = fb.cpu().numpy()[(50 + np.arange(nrows)) & 63].astype(np.float64)
+    assert np.max(np.abs(got - ref) / np.abs(ref)) <= 1e-5
+
+
+def test_channelise_fill_frames(vf, O):
+    """Slots marked -1 are zero-byte fill frames (PIPE:1044-1052)."""
+    torch = _torch()
+    buf = _frames(0.02, seed=7)
+    L = vf.layout(nave=1, muoslowfreq=384.0)
+    Lo = O.Layout(nave=1, muoslowfreq=384.0)
+    p0, p1 = [x.copy() for x in _pol_streams(buf.numpy())]
+    nslots = len(p0) // 5000
+    holes = [3, 4, 17]
+    for h in holes:
+        p0[h * 5000:(h + 1) * 5000] = 0
+    p1[9 * 5000:10 * 5000] = 0
+    nrows = len(p0) // 12500
+    ref = O.channelise(p0, p1, Lo)[:nrows]
+    dev = torch.device("cuda")
+    idx = torch.arange(nslots, dtype=torch.int64)
+    s0 = idx * (2 * 5032) + 32
+    s1 = s0 + 5032
+    s0[holes] = -1
+    s1[9] = -1
+    fb = vf.channelise(buf.to(dev), s0.to(dev), s1.to(dev), 0, nrows, L)
+    torch.cuda.synchronize()
+    assert np.max(np.abs(fb.cpu().numpy() - ref) / np.abs(ref)) <= 1e-5
+
+
+def _rand_fb(rows, nch, seed=1):
+    rng = np.random.default_rng(seed)
+    base = rng.uniform(200, 900, nch)
+    cal = 1.0 + 0.2 * ((np.arange(rows) // 128) % 2)
+    return (rng.chisquare(20, (rows, nch)) / 20.0 * base[None, :] * cal[:, None]).astype(np.float32)
+
+
+@pytest.mark.parametrize("rows", [128 * 5, 128 * 5 + 60, 129])
+def test_bandpass_matches_fp64(vf, O, rows):
+    torch = _torch()
+    nch = 100
+    x = _rand_fb(rows, nch)
+    x[5, 7] = 1e5  # an outlier the clip must reject
+    ref = O.subtract_bp_cal(x.astype(np.float64))
+    dev = torch.device("cuda")
+    out = vf.bandpass(torch.from_numpy(x).to(dev))
+    tm = torch.empty((rows, nch), device=dev)
+    out2 = vf.bandpass(torch.from_numpy(x).to(dev), tm_out=tm)
+    torch.cuda.synchronize()
+    got = out.cpu().numpy().T.astype(np.float64)
+    tol = 1e-6 * np.abs(x).max()
+    assert np.max(np.abs(got - ref)) <= tol
+    assert np.array_equal(out.cpu().numpy(), out2.cpu().numpy())
+    assert np.max(np.abs(tm.cpu().numpy() - ref)) <= tol
+
+
+def test_bandpass_ring_in_and_out(vf, O):
+    torch = _torch()
+    rows, nch = 256, 40
+    x = _rand_fb(rows, nch, seed=9)
+    ref = O.subtract_bp_cal(x.astype(np.float64))
+    dev = torch.device("cuda")
+    ring_in = torch.zeros((512, nch), device=dev)
+    ridx = (400 + np.arange(rows)) & 511
+    ring_in[torch.from_numpy(ridx).to(dev)] = torch.from_numpy(x).to(dev)
+    ring_out = torch.zeros((nch, 1024), device=dev)
+    vf.bandpass(ring_in, nrows=rows, in_row0=400, in_row_mask=511, out=ring_out, out_row0=900, out_row_mask=1023)
+    torch.cuda.synchronize()
+    got = ring_out.cpu().numpy()[:, (900 + np.arange(rows)) & 1023].T
+    assert np.max(np.abs(got - ref)) <= 1e-6 * np.abs(x).max()
+
+
+def _dd_case(ndm=40, nch=256, nt=1000, seed=2, dm_max=30.0):
+    rng = np.random.default_rng(seed)
+    fch1, chanbw, tchan = 384.0, 0.25, 0.001
+    from vfrb_oracle import delay_table
+    dms = np.linspace(0, dm_max, ndm).astype(np.float32)
+    off, md = delay_table(dms, fch1, chanbw, tchan, nch)
+    md = int(off.max())
+    fb = rng.standard_normal((nt + md, nch)).astype(np.float32) * 3.0
+    return dms, off, md, fb
+
+
+def test_dedisperse_and_calcstats_match_fp64(vf, O):
+    torch = _torch()
+    dms, off, md, fb = _dd_case()
+    nt = 1000
+    # a pulse at DM index 23
+    for c in range(fb.shape[1]):
+        fb[400 + off[23, c], c] += 8.0
+    ref = O.dedisperse(fb.astype(np.float64), off, nt)
+    st_ref = O.calcstats_dm(ref)
+    plan = vf.DedispPlan(off)
+    dev = torch.device("cuda")
+    fb_cm = torch.from_numpy(np.ascontiguousarray(fb.T)).to(dev)
+    out, st = plan(fb_cm, nt)
+    torch.cuda.synchronize()
+    got = out.cpu().numpy().astype(np.float64)
+    rms = np.sqrt(np.mean(ref ** 2))
+    e = np.max(np.abs(got - ref)) / rms
+    print("dedisperse max err / rms", e)
+    assert e <= 1e-5
+    for k in ("ave", "sigma"):
+        g = st[k].cpu().numpy().astype(np.float64)
+        r = st_ref[k].astype(np.float64)
+        assert np.max(np.abs(g - r) / np.maximum(np.abs(r), 1e-30)) <= 1e-5 or np.max(np.abs(g - r)) <= 1e-6 * rms
+    pk = st["peak"].cpu().numpy()
+    assert np.max(np.abs(pk - st_ref["peak"]) / np.maximum(st_ref["peak"], 1e-3)) <= 1e-4
+    assert np.array_equal(st["frb"].cpu().numpy(), st_ref["frb"])
+    assert int(st["argmax"].cpu().numpy()[23]) == 400
+    assert np.array_equal(st["argmax"].cpu().numpy(), st_ref["argmax"])
+
+
+def test_dedisperse_wide_spread_uses_direct_path(vf, O):
+    """A DM list with a huge jump cannot be staged; the direct path must agree."""
+    torch = _torch()
+    rng = np.random.default_rng(4)
+    nch, nt = 64, 300
+    off = np.zeros((3, nch), np.int32)
+    off[1] = np.arange(nch) * 2
+    off[2] = np.arange(nch) * 500  # 31500-row spread
+    md = int(off.max())
+    fb = rng.standard_normal((nt + md, nch)).astype(np.float32)
+    ref = O.dedisperse(fb.astype(np.float64), off, nt)
+    plan = vf.DedispPlan(off)
+    out, _ = plan(torch.from_numpy(np.ascontiguousarray(fb.T)).cuda(), nt)
+    torch.cuda.synchronize()
+    assert np.max(np.abs(out.cpu().numpy() - ref)) <= 1e-5 * np.sqrt(np.mean(ref ** 2))
+
+
+def test_dedisperse_ring_wrap(vf, O):
+    torch = _torch()
+    dms, off, md, fb = _dd_case(ndm=20, nch=128, nt=700, seed=8)
+    nt = 700
+    rows = fb.shape[0]
+    R = 1 << int(np.ceil(np.log2(rows + 1)))
+    r0 = R - 300  # wraps
+    ring = np.zeros((fb.shape[1], R), np.float32)
+    ring[:, (r0 + np.arange(rows)) & (R - 1)] = fb.T
+    ref = O.dedisperse(fb.astype(np.float64), off, nt)
+    plan = vf.DedispPlan(off)
+    out, _ = plan(torch.from_numpy(ring).cuda(), nt, row0=r0, row_mask=R - 1, nrows_valid=rows)
+    torch.cuda.synchronize()
+    assert np.max(np.abs(out.cpu().numpy() - ref)) <= 1e-5 * np.sqrt(np.mean(ref ** 2))
+
+
+def test_dedisperse_sigma_matches_fp64(vf, O):
+    """dedisperseSTATS (TS:1450-1481)."""
+    torch = _torch()
+    dms, off, md, fb = _dd_case(ndm=2, nch=384, nt=900, seed=11)
+    nt = 900
+    ave_ref, sig_ref = O.dedisperse_sigma(fb.astype(np.float64), off, nt)
+    plan = vf.DedispPlan(off)
+    sig = torch.empty((2, nt), device="cuda")
+    out, _ = plan(torch.from_numpy(np.ascontiguousarray(fb.T)).cuda(), nt, sigma_out=sig, stats=False)
+    torch.cuda.synchronize()
+    assert np.max(np.abs(out.cpu().numpy() - ave_ref)) <= 1e-5 * np.sqrt(np.mean(ave_ref ** 2))
+    assert np.max(np.abs(sig.cpu().numpy() - sig_ref) / sig_ref) <= 1e-5
+
+
+@pytest.mark.parametrize("storage,tol", [(1, 3e-3), (2, 1.2e-1)])
+def test_reduced_precision_storage(vf, O, storage, tol):
+    """FP16 / int8 storage of z = (P - mean)/s_c with FP32 accumulation of s_c*z."""
+    torch = _torch()
+    rows, nch = 128 * 12, 256
+    raw = _rand_fb(rows, nch, seed=21)
+    bp = O.subtract_bp_cal(raw.astype(np.float64))
+    from vfrb_oracle import delay_table
+    dms = np.linspace(0, 20, 24).astype(np.float32)
+    off, _ = delay_table(dms, 384.0, 0.25, 0.001, nch)
+    md = int(off.max())
+    nt = rows - md
+    ref = O.dedisperse(bp, off, nt)
+    s = np.sqrt(np.var(bp[:128], axis=0, ddof=1)).astype(np.float32)
+    q = 16.0
+    dev = torch.device("cuda")
+    inv = torch.from_numpy(1.0 / s).to(dev)
+    w = s / (q if storage == 2 else 1.0)
+    fbz = vf.bandpass(torch.from_numpy(raw).to(dev), storage=storage, inv_scale=inv, q_scale=q)
+    plan = vf.DedispPlan(off)
+    out, _ = plan(fbz, nt, storage=storage, chan_scale=torch.from_numpy(w.astype(np.float32)).to(dev))
+    out32, _ = plan(vf.bandpass(torch.from_numpy(raw).to(dev)), nt)
+    torch.cuda.synchronize()
+    rms = np.sqrt(np.mean(ref ** 2))
+    e = np.max(np.abs(out.cpu().numpy() - ref)) / rms
+    e32 = np.max(np.abs(out32.cpu().numpy() - ref)) / rms
+    print(f"storage {storage}: max err/rms {e:.3e} (fp32 {e32:.3e})")
+    assert e <= tol
+
+
+def test_chan_stats_matches_fp64(vf, O):
+    torch = _torch()
+    rows, nch = 1700, 90
+    x = _rand_fb(rows, nch, seed=13)
+    bp = O.subtract_bp_cal(x.astype(np.float64)).astype(np.float32)
+    a_r, s_r, o_r = O.calcstats_chan(bp.astype(np.float64), 500, 4)
+    dev = torch.device("cuda")
+    a, s, o = vf.chan_stats(torch.from_numpy(np.ascontiguousarray(bp.T)).to(dev), rows, 500, 4)
+    torch.cuda.synchronize()
+    assert np.max(np.abs(a.cpu().numpy() - a_r)) <= 1e-6 * np.abs(bp).max()
+    assert np.max(np.abs(s.cpu().numpy() - s_r) / s_r) <= 1e-6
+    assert np.array_equal(o.cpu().numpy(), o_r)
+
+
+def test_transpose(vf):
+    torch = _torch()
+    x = torch.randn(70, 333, device="cuda")
+    y = vf.fb_to_time_major(x)
+    torch.cuda.synchronize()
+    assert torch.equal(y, x.t())

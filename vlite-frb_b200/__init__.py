@@ -1,0 +1,271 @@
+"""vlite-frb-b200: ctypes binding of libvfrb (the sm_100a FRB search chain).
+
+The binding is thin: every call goes through the C ABI declared in
+``include/vfrb.h``.  Device buffers are torch CUDA tensors (torch provides
+device memory and streams only).  There is no CPU fallback: importing the
+module on a machine without ``lib/libvfrb.so`` raises, and every stage call
+raises ``VfrbError`` on a non-zero status.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "lib", "libvfrb.so")
+
+VFRB_OK, VFRB_EOD, VFRB_ERR = 0, 1, 2
+F32, F16, I8 = 0, 1, 2
+
+
+class VfrbError(RuntimeError):
+    def __init__(self, status: int, what: str = ""):
+        self.status = status
+        msg = _lib.vfrb_strerror(status).decode() if _lib is not None else str(status)
+        super().__init__(f"{what}: status {status} ({msg})")
+
+
+def _load():
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(f"libvfrb.so not built ({LIB_PATH}); run vlite-frb_b200/build.py")
+    return C.CDLL(LIB_PATH)
+
+
+_lib = None
+_lib = _load()
+
+
+def lib():
+    return _lib
+
+
+# ---- structures (mirror include/vfrb.h) --------------------------------------
+class Hdr(C.Structure):
+    _fields_ = [(n, C.c_uint32) for n in (
+        "seconds", "legacymode", "invalid", "frame", "epoch", "unassigned", "framelength8", "nchan_log2",
+        "version", "stationid", "threadid", "nbits_minus1", "iscomplex", "eversion", "extended1",
+        "extended2", "extended3", "extended4")]
+
+
+class Layout(C.Structure):
+    _fields_ = [(n, C.c_int32) for n in (
+        "twonchan", "nchan", "nfreq", "nchanout", "nskip", "nave", "nbundle", "nloop", "maxnt", "nhalfcyc")] + [
+        ("chanbw", C.c_double), ("fch1", C.c_double), ("foff", C.c_double), ("tchan", C.c_double),
+        ("maxtime", C.c_float)]
+
+
+class ChanArgs(C.Structure):
+    _fields_ = [("frames", C.c_void_p), ("slots0", C.c_void_p), ("slots1", C.c_void_p), ("nslots", C.c_int64),
+                ("sample0", C.c_int64), ("nrows", C.c_int32), ("twonchan", C.c_int32), ("nave", C.c_int32),
+                ("nfreq", C.c_int32), ("nskip", C.c_int32), ("nchanout", C.c_int32), ("out", C.c_void_p),
+                ("out_row_stride", C.c_int64), ("out_row0", C.c_int64), ("out_row_mask", C.c_uint32),
+                ("d_err", C.c_void_p)]
+
+
+class BpArgs(C.Structure):
+    _fields_ = [("inp", C.c_void_p), ("in_row_stride", C.c_int64), ("in_row0", C.c_int64),
+                ("in_row_mask", C.c_uint32), ("nchan", C.c_int32), ("nrows", C.c_int32), ("window", C.c_int32),
+                ("storage", C.c_int32), ("out", C.c_void_p), ("out_chan_stride", C.c_int64),
+                ("out_row0", C.c_int64), ("out_row_mask", C.c_uint32), ("inv_scale", C.c_void_p),
+                ("q_scale", C.c_float), ("win_mean", C.c_void_p), ("win_var", C.c_void_p), ("tm_out", C.c_void_p),
+                ("tm_row_stride", C.c_int64), ("d_err", C.c_void_p)]
+
+
+class DdArgs(C.Structure):
+    _fields_ = [("fb", C.c_void_p), ("storage", C.c_int32), ("chan_scale", C.c_void_p),
+                ("chan_stride", C.c_int64), ("row0", C.c_int64), ("row_mask", C.c_uint32),
+                ("nrows_valid", C.c_int64), ("nt_out", C.c_int64), ("out", C.c_void_p), ("out_stride", C.c_int64),
+                ("sigma_out", C.c_void_p), ("workspace", C.c_void_p), ("workspace_bytes", C.c_size_t),
+                ("ave", C.c_void_p), ("sigma", C.c_void_p), ("peak", C.c_void_p), ("frb", C.c_void_p),
+                ("argmax", C.c_void_p), ("d_err", C.c_void_p)]
+
+
+class CsArgs(C.Structure):
+    _fields_ = [("fb", C.c_void_p), ("chan_stride", C.c_int64), ("row0", C.c_int64), ("row_mask", C.c_uint32),
+                ("nchan", C.c_int32), ("nrows", C.c_int32), ("ncolstatblk", C.c_int32), ("nstatblks", C.c_int32),
+                ("ave", C.c_void_p), ("sig", C.c_void_p), ("outlier", C.c_void_p)]
+
+
+_lib.vfrb_strerror.restype = C.c_char_p
+_lib.vfrb_strerror.argtypes = [C.c_int]
+_lib.vfrb_decode_header.argtypes = [C.c_char_p, C.POINTER(Hdr)]
+_lib.vfrb_header_dmjd.restype = C.c_double
+_lib.vfrb_header_dmjd.argtypes = [C.POINTER(Hdr), C.c_int]
+_lib.vfrb_layout_init.argtypes = [C.POINTER(Layout), C.c_int, C.c_int, C.c_int, C.c_double, C.c_int, C.c_float]
+_lib.vfrb_delay_table.argtypes = [C.POINTER(Layout), C.c_void_p, C.c_int, C.c_void_p, C.POINTER(C.c_int32)]
+for _n, _t in (("vfrb_channelise", ChanArgs), ("vfrb_bandpass", BpArgs), ("vfrb_chan_stats", CsArgs)):
+    getattr(_lib, _n).argtypes = [C.POINTER(_t), C.c_void_p]
+_lib.vfrb_ddplan_create.argtypes = [C.POINTER(C.c_void_p), C.c_void_p, C.c_int, C.c_int]
+_lib.vfrb_ddplan_destroy.argtypes = [C.c_void_p]
+_lib.vfrb_ddplan_max_delay.argtypes = [C.c_void_p]
+_lib.vfrb_dedisperse_workspace_bytes.restype = C.c_size_t
+_lib.vfrb_dedisperse_workspace_bytes.argtypes = [C.c_void_p, C.c_int64]
+_lib.vfrb_dedisperse.argtypes = [C.c_void_p, C.POINTER(DdArgs), C.c_void_p]
+_lib.vfrb_fb_to_time_major.argtypes = [C.c_void_p, C.c_int64, C.c_int64, C.c_uint32, C.c_int, C.c_int, C.c_void_p,
+                                       C.c_int64, C.c_void_p]
+
+
+def _check(st: int, what: str):
+    if st != 0:
+        raise VfrbError(st, what)
+
+
+# ---- host helpers -------------------------------------------------------------
+def decode_header(b: bytes) -> dict:
+    h = Hdr()
+    _check(_lib.vfrb_decode_header(bytes(b[:32]), C.byref(h)), "vfrb_decode_header")
+    return {n: getattr(h, n) for n, _ in Hdr._fields_}
+
+
+def header_dmjd(b: bytes, fps: int = 25600) -> float:
+    h = Hdr()
+    _check(_lib.vfrb_decode_header(bytes(b[:32]), C.byref(h)), "vfrb_decode_header")
+    return _lib.vfrb_header_dmjd(C.byref(h), fps)
+
+
+def layout(twonchan=12500, nave=4, nbundle=32, muoslowfreq=360.0, nchanout_fixed=0, maxtime=70.0) -> Layout:
+    L = Layout()
+    _check(_lib.vfrb_layout_init(C.byref(L), twonchan, nave, nbundle, muoslowfreq, nchanout_fixed, maxtime),
+           "vfrb_layout_init")
+    return L
+
+
+def delay_table(L: Layout, dms) -> tuple[np.ndarray, int]:
+    d = np.ascontiguousarray(dms, dtype=np.float32)
+    off = np.zeros((len(d), L.nchanout), np.int32)
+    md = C.c_int32(0)
+    _check(_lib.vfrb_delay_table(C.byref(L), d.ctypes.data, len(d), off.ctypes.data, C.byref(md)),
+           "vfrb_delay_table")
+    return off, int(md.value)
+
+
+# ---- device stage wrappers (torch tensors) ---------------------------------------
+def _torch():
+    import torch  # noqa: WPS433  (torch only provides device memory and streams)
+    return torch
+
+
+def _ptr(t):
+    return None if t is None else C.c_void_p(t.data_ptr())
+
+
+def _stream(stream=None):
+    torch = _torch()
+    s = stream if stream is not None else torch.cuda.current_stream()
+    return C.c_void_p(s.cuda_stream)
+
+
+def contiguous_slots(nbytes_per_pol: int, device, base0: int = 0, base1: int | None = None):
+    """Slot tables for two contiguous per-pol byte arrays (payloads back to back)."""
+    torch = _torch()
+    n = (nbytes_per_pol + 4999) // 5000
+    s = torch.arange(n, dtype=torch.int64, device=device) * 5000
+    return s + base0, s + (base1 if base1 is not None else base0)
+
+
+def channelise(frames, slots0, slots1, sample0: int, nrows: int, L: Layout, out=None, out_row0=0,
+               out_row_mask=0xFFFFFFFF, d_err=None, stream=None):
+    torch = _torch()
+    if out is None:
+        out = torch.empty((nrows, L.nchanout), dtype=torch.float32, device=frames.device)
+    a = ChanArgs(frames=frames.data_ptr(), slots0=slots0.data_ptr(), slots1=slots1.data_ptr(),
+                 nslots=slots0.numel(), sample0=sample0, nrows=nrows, twonchan=L.twonchan, nave=L.nave,
+                 nfreq=L.nfreq, nskip=L.nskip, nchanout=L.nchanout, out=out.data_ptr(),
+                 out_row_stride=out.stride(0), out_row0=out_row0, out_row_mask=out_row_mask,
+                 d_err=d_err.data_ptr() if d_err is not None else None)
+    _check(_lib.vfrb_channelise(C.byref(a), _stream(stream)), "vfrb_channelise")
+    return out
+
+
+def bandpass(fb_tm, nrows=None, storage=F32, out=None, out_row0=0, out_row_mask=0xFFFFFFFF, inv_scale=None,
+             q_scale=16.0, in_row0=0, in_row_mask=0xFFFFFFFF, window=128, win_mean=None, win_var=None,
+             tm_out=None, d_err=None, stream=None):
+    torch = _torch()
+    nrows = fb_tm.shape[0] if nrows is None else nrows
+    nchan = fb_tm.shape[1]
+    if out is None:
+        dt = {F32: torch.float32, F16: torch.float16, I8: torch.int8}[storage]
+        out = torch.empty((nchan, nrows), dtype=dt, device=fb_tm.device)
+    a = BpArgs(inp=fb_tm.data_ptr(), in_row_stride=fb_tm.stride(0), in_row0=in_row0, in_row_mask=in_row_mask,
+               nchan=nchan, nrows=nrows, window=window, storage=storage, out=out.data_ptr(),
+               out_chan_stride=out.stride(0), out_row0=out_row0, out_row_mask=out_row_mask,
+               inv_scale=_ptr(inv_scale), q_scale=q_scale, win_mean=_ptr(win_mean), win_var=_ptr(win_var),
+               tm_out=_ptr(tm_out), tm_row_stride=tm_out.stride(0) if tm_out is not None else 0,
+               d_err=_ptr(d_err))
+    _check(_lib.vfrb_bandpass(C.byref(a), _stream(stream)), "vfrb_bandpass")
+    return out
+
+
+class DedispPlan:
+    """Device copy of a delay table [ndm][nchan] (vfrb_ddplan)."""
+
+    def __init__(self, offsets: np.ndarray):
+        off = np.ascontiguousarray(offsets, dtype=np.int32)
+        self.ndm, self.nchan = off.shape
+        p = C.c_void_p()
+        _check(_lib.vfrb_ddplan_create(C.byref(p), off.ctypes.data, self.ndm, self.nchan), "vfrb_ddplan_create")
+        self._p = p
+        self.max_delay = _lib.vfrb_ddplan_max_delay(p)
+
+    def workspace_bytes(self, nt_out: int) -> int:
+        return int(_lib.vfrb_dedisperse_workspace_bytes(self._p, nt_out))
+
+    def __call__(self, fb_cm, nt_out: int, storage=F32, chan_scale=None, row0=0, row_mask=0xFFFFFFFF,
+                 nrows_valid=None, out=None, sigma_out=None, stats=True, workspace=None, d_err=None, stream=None):
+        torch = _torch()
+        dev = fb_cm.device
+        if out is None:
+            out = torch.empty((self.ndm, nt_out), dtype=torch.float32, device=dev)
+        st = {}
+        if stats:
+            st = dict(ave=torch.empty(self.ndm, dtype=torch.float32, device=dev),
+                      sigma=torch.empty(self.ndm, dtype=torch.float32, device=dev),
+                      peak=torch.empty(self.ndm, dtype=torch.float32, device=dev),
+                      frb=torch.empty(self.ndm, dtype=torch.int32, device=dev),
+                      argmax=torch.empty(self.ndm, dtype=torch.int32, device=dev))
+            if workspace is None:
+                workspace = torch.empty(max(1, self.workspace_bytes(nt_out)), dtype=torch.uint8, device=dev)
+        a = DdArgs(fb=fb_cm.data_ptr(), storage=storage, chan_scale=_ptr(chan_scale), chan_stride=fb_cm.stride(0),
+                   row0=row0, row_mask=row_mask,
+                   nrows_valid=fb_cm.shape[1] if nrows_valid is None else nrows_valid, nt_out=nt_out,
+                   out=out.data_ptr(), out_stride=out.stride(0), sigma_out=_ptr(sigma_out),
+                   workspace=_ptr(workspace), workspace_bytes=workspace.numel() if workspace is not None else 0,
+                   ave=_ptr(st.get("ave")), sigma=_ptr(st.get("sigma")), peak=_ptr(st.get("peak")),
+                   frb=_ptr(st.get("frb")), argmax=_ptr(st.get("argmax")), d_err=_ptr(d_err))
+        _check(_lib.vfrb_dedisperse(self._p, C.byref(a), _stream(stream)), "vfrb_dedisperse")
+        return out, st
+
+    def __del__(self):
+        try:
+            if getattr(self, "_p", None):
+                _lib.vfrb_ddplan_destroy(self._p)
+                self._p = None
+        except Exception:
+            pass
+
+
+def chan_stats(fb_cm, nrows: int, ncolstatblk: int, nstatblks: int, row0=0, row_mask=0xFFFFFFFF, stream=None):
+    torch = _torch()
+    nchan = fb_cm.shape[0]
+    dev = fb_cm.device
+    ave = torch.empty((nstatblks, nchan), dtype=torch.float32, device=dev)
+    sig = torch.empty_like(ave)
+    outl = torch.empty_like(ave)
+    a = CsArgs(fb=fb_cm.data_ptr(), chan_stride=fb_cm.stride(0), row0=row0, row_mask=row_mask, nchan=nchan,
+               nrows=nrows, ncolstatblk=ncolstatblk, nstatblks=nstatblks, ave=ave.data_ptr(), sig=sig.data_ptr(),
+               outlier=outl.data_ptr())
+    _check(_lib.vfrb_chan_stats(C.byref(a), _stream(stream)), "vfrb_chan_stats")
+    return ave, sig, outl
+
+
+def fb_to_time_major(fb_cm, nrows=None, row0=0, row_mask=0xFFFFFFFF, out=None, stream=None):
+    torch = _torch()
+    nchan = fb_cm.shape[0]
+    nrows = fb_cm.shape[1] if nrows is None else nrows
+    if out is None:
+        out = torch.empty((nrows, nchan), dtype=torch.float32, device=fb_cm.device)
+    _check(_lib.vfrb_fb_to_time_major(fb_cm.data_ptr(), fb_cm.stride(0), row0, row_mask, nchan, nrows,
+                                      out.data_ptr(), out.stride(0), _stream(stream)), "vfrb_fb_to_time_major")
+    return out

@@ -1,0 +1,492 @@
+// K3: brute-force incoherent dedispersion + fused per-DM statistics (sm_100a).
+//
+// Replaces dedisp_execute (PIPE:671) by the reference's in-tree sum
+// (PIPE:1517-1537) and fuses calcstats (PIPE:1337-1370); the SIGMA variant
+// is dedisperseSTATS (TS:1450-1481).
+//
+// Tiling: a CTA owns a block of 16 DM trials x 256 output samples.  For each
+// chunk of channels it stages, per channel, the contiguous run of rows that
+// any of its 16 DMs touches (256 + the chunk's delay spread) from the
+// channel-major filterbank into shared memory with 16-byte vector loads; the
+// 16 trials then all read their shifted windows from that one copy (reuse
+// across neighbouring DM trials).  Lanes run along time, so every shared
+// memory read of a warp is 32 consecutive elements (conflict free) and the
+// per-channel delay is warp-uniform.  Accumulation is FP32 in registers; the
+// FP16 / int8 forms apply the per-channel weight with an FMA.
+#include "vfrb_common.cuh"
+
+#include <algorithm>
+#include <vector>
+
+namespace vfrb {
+
+constexpr int kDdThreads = 256;
+constexpr int kDdDm = 16;          // DM trials per CTA
+constexpr int kDdDmPerWarp = kDdDm / (kDdThreads / 32);
+constexpr int kDdPerLane = 8;      // output samples per lane
+constexpr int kDdNt = 32 * kDdPerLane;  // 256 output samples per CTA
+constexpr int kDdSmemBudget = 96 * 1024;
+constexpr int kDdMaxChunk = 32;
+
+struct DmPartial {
+  double s, s2;
+  float mx;
+  int arg;
+};
+
+struct DdKParams {
+  const void* fb;
+  const float* chan_scale;
+  long long chan_stride;
+  long long row0;
+  unsigned row_mask;
+  long long nrows_valid;
+  int nchan;
+  const int* off;
+  int ndm;
+  long long nt_out;
+  float* out;
+  long long out_stride;
+  float* sig_out;
+  DmPartial* part;
+  int chunk;
+  int lmax;
+  int* err;
+};
+
+template <typename T> struct Vec;
+template <> struct Vec<float> { static constexpr int n = 4; };
+template <> struct Vec<__half> { static constexpr int n = 8; };
+template <> struct Vec<int8_t> { static constexpr int n = 16; };
+
+template <typename T> __device__ __forceinline__ float to_f(T v);
+template <> __device__ __forceinline__ float to_f<float>(float v) { return v; }
+template <> __device__ __forceinline__ float to_f<__half>(__half v) { return __half2float(v); }
+template <> __device__ __forceinline__ float to_f<int8_t>(int8_t v) { return (float)v; }
+
+__device__ __forceinline__ double wsum(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+template <typename T, bool SIGMA>
+__global__ void __launch_bounds__(kDdThreads) k_dedisperse(const DdKParams p) {
+  constexpr int VEC = Vec<T>::n;
+  extern __shared__ float4 sm4[];
+  const int CH = p.chunk;
+  int* s_off = reinterpret_cast<int*>(sm4);            // [kDdDm][CH]
+  long long* s_abs = reinterpret_cast<long long*>(s_off + kDdDm * CH);  // [CH] first staged row (8-byte aligned: 16*CH ints)
+  float* s_w = reinterpret_cast<float*>(s_abs + CH);    // [CH]
+  T* tile = reinterpret_cast<T*>(sm4 + ((kDdDm * CH * 4 + CH * 8 + CH * 4 + 8 * 4 + 15) / 16));
+
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const long long t0 = (long long)blockIdx.x * kDdNt;
+  const int d0 = blockIdx.y * kDdDm;
+  const T* fb = reinterpret_cast<const T*>(p.fb);
+  int err = 0;
+
+  float acc[kDdDmPerWarp][kDdPerLane];
+  float acc2[SIGMA ? kDdDmPerWarp : 1][SIGMA ? kDdPerLane : 1];
+#pragma unroll
+  for (int j = 0; j < kDdDmPerWarp; ++j)
+#pragma unroll
+    for (int k = 0; k < kDdPerLane; ++k) {
+      acc[j][k] = 0.f;
+      if (SIGMA) acc2[j][k] = 0.f;
+    }
+
+  for (int c0 = 0; c0 < p.nchan; c0 += CH) {
+    const int nc = min(CH, p.nchan - c0);
+    for (int i = tid; i < kDdDm * CH; i += kDdThreads) {
+      const int dl = i / CH, cl = i - dl * CH;
+      const int d = min(d0 + dl, p.ndm - 1);
+      s_off[i] = (cl < nc) ? __ldg(p.off + (long long)d * p.nchan + c0 + cl) : 0;
+    }
+    __syncthreads();
+    for (int cl = tid; cl < CH; cl += kDdThreads) {
+      int mn = 0x7fffffff, mx = -0x7fffffff;
+#pragma unroll
+      for (int dl = 0; dl < kDdDm; ++dl) {
+        const int o = s_off[dl * CH + cl];
+        mn = min(mn, o);
+        mx = max(mx, o);
+      }
+      const long long a0 = (p.row0 + t0 + mn) & ~(long long)(VEC - 1);
+      if (p.row0 + t0 + mx + kDdNt - a0 > p.lmax) err |= kErrOffsetRange;
+      s_abs[cl] = a0;
+      s_w[cl] = (p.chan_scale && cl < nc) ? p.chan_scale[c0 + cl] : 1.f;
+    }
+    __syncthreads();
+    // stage rows [s_abs, s_abs + lmax) of each channel of the chunk
+    const int nvec = p.lmax / VEC;
+    for (int cl = warp; cl < nc; cl += kDdThreads / 32) {
+      const T* src = fb + (long long)(c0 + cl) * p.chan_stride;
+      const long long a0 = s_abs[cl];
+      uint4* dst = reinterpret_cast<uint4*>(tile + (long long)cl * p.lmax);
+      for (int v = lane; v < nvec; v += 32) {
+        const long long r = a0 + (long long)v * VEC;  // absolute (unmasked) row
+        uint4 val = make_uint4(0, 0, 0, 0);
+        if (r >= p.row0 && r + VEC <= p.row0 + p.nrows_valid) {
+          const unsigned long long rr = (unsigned long long)r & (unsigned long long)p.row_mask;
+          val = __ldg(reinterpret_cast<const uint4*>(src + rr));
+        } else if (r + VEC > p.row0 && r < p.row0 + p.nrows_valid) {
+          // partially valid vector at the edge of the valid rows
+          union {
+            uint4 u;
+            T t[VEC];
+          } tmp;
+          tmp.u = make_uint4(0, 0, 0, 0);
+#pragma unroll
+          for (int e = 0; e < VEC; ++e) {
+            const long long re = r + e;
+            if (re >= p.row0 && re < p.row0 + p.nrows_valid)
+              tmp.t[e] = src[(unsigned long long)re & (unsigned long long)p.row_mask];
+          }
+          val = tmp.u;
+        }
+        dst[v] = val;
+      }
+    }
+    __syncthreads();
+#pragma unroll 2
+    for (int cl = 0; cl < nc; ++cl) {
+      const T* trow = tile + (long long)cl * p.lmax;
+      const float wc = s_w[cl];
+#pragma unroll
+      for (int j = 0; j < kDdDmPerWarp; ++j) {
+        const int dl = warp * kDdDmPerWarp + j;
+        int o = (int)(p.row0 + t0 + s_off[dl * CH + cl] - s_abs[cl]);
+        o = min(max(o, 0), p.lmax - kDdNt) + lane;  // never leaves the tile, even for a bad table
+#pragma unroll
+        for (int k = 0; k < kDdPerLane; ++k) {
+          const float v = to_f<T>(trow[o + 32 * k]);
+          if (sizeof(T) == 4) {
+            acc[j][k] += v;
+          } else {
+            acc[j][k] = fmaf(wc, v, acc[j][k]);
+          }
+          if (SIGMA) acc2[j][k] = fmaf(v, v, acc2[j][k]);
+        }
+      }
+    }
+    __syncthreads();
+  }
+
+  // epilogue: out = sum / NCHANOUT (PIPE:1534), and calcstats partials
+  const float fn = (float)p.nchan;
+#pragma unroll
+  for (int j = 0; j < kDdDmPerWarp; ++j) {
+    const int d = d0 + warp * kDdDmPerWarp + j;
+    if (d >= p.ndm) continue;  // warp-uniform
+    double s = 0.0, s2 = 0.0;
+    float mx = -INFINITY;
+    int arg = 0x7fffffff;
+#pragma unroll
+    for (int k = 0; k < kDdPerLane; ++k) {
+      const long long t = t0 + lane + 32 * k;
+      if (t < p.nt_out) {
+        const float val = acc[j][k] / fn;
+        p.out[(long long)d * p.out_stride + t] = val;
+        if (SIGMA) {
+          // sigma = sqrt((sum d^2 - (sum d)^2) / (N (N-1))), d = x - mean (TS:1468-1477)
+          const double n = (double)p.nchan;
+          const double sx = (double)acc[j][k], sxx = (double)acc2[j][k];
+          double var = (sxx - sx * sx / n) / (n * (n - 1.0));
+          p.sig_out[(long long)d * p.out_stride + t] = (float)sqrt(var > 0.0 ? var : 0.0);
+        }
+        s += (double)val;
+        s2 += (double)val * (double)val;
+        if (val > mx) {
+          mx = val;
+          arg = (int)t;
+        }
+      }
+    }
+    s = wsum(s);
+    s2 = wsum(s2);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      const float omx = __shfl_xor_sync(0xffffffffu, mx, o);
+      const int oarg = __shfl_xor_sync(0xffffffffu, arg, o);
+      if (omx > mx || (omx == mx && oarg < arg)) {
+        mx = omx;
+        arg = oarg;
+      }
+    }
+    if (lane == 0 && p.part) {
+      DmPartial q;
+      q.s = s;
+      q.s2 = s2;
+      q.mx = mx;
+      q.arg = arg;
+      p.part[(long long)blockIdx.x * p.ndm + d] = q;
+    }
+  }
+  if (err && p.err) atomicOr(p.err, err);
+}
+
+// calcstats finalize: one warp per DM reduces the time-block partials.
+__global__ void __launch_bounds__(256) k_dm_stats(const DmPartial* __restrict__ part, int ntb, int ndm,
+                                                  long long nt_out, float* ave, float* sigma, float* peak,
+                                                  int* frb, int* argmax) {
+  const int lane = threadIdx.x & 31;
+  const int d = blockIdx.x * 8 + (threadIdx.x >> 5);
+  if (d >= ndm) return;
+  double s = 0.0, s2 = 0.0;
+  float mx = -INFINITY;
+  int arg = 0x7fffffff;
+  for (int b = lane; b < ntb; b += 32) {
+    const DmPartial q = part[(long long)b * ndm + d];
+    s += q.s;
+    s2 += q.s2;
+    if (q.mx > mx || (q.mx == mx && q.arg < arg)) {
+      mx = q.mx;
+      arg = q.arg;
+    }
+  }
+  s = wsum(s);
+  s2 = wsum(s2);
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    const float omx = __shfl_xor_sync(0xffffffffu, mx, o);
+    const int oarg = __shfl_xor_sync(0xffffffffu, arg, o);
+    if (omx > mx || (omx == mx && oarg < arg)) {
+      mx = omx;
+      arg = oarg;
+    }
+  }
+  if (lane != 0) return;
+  const double n = (double)nt_out;
+  const double tave = s / n;
+  const double tsig = (s2 - s * s / n) / (n - 1.0);  // == the reference's corrected two-pass form
+  const float ave_f = (float)tave;
+  const float sig_f = (float)sqrt(tsig);
+  // max_t (x - ave)/sigma in float equals f(max_t x): the map is monotone.
+  const float snr = (mx - ave_f) / sig_f;
+  if (ave) ave[d] = ave_f;
+  if (sigma) sigma[d] = sig_f;
+  if (peak) peak[d] = (snr > 0.f) ? snr : 0.f;
+  if (frb) frb[d] = (snr > 3.0f) ? 1 : 0;
+  if (argmax) argmax[d] = arg;
+}
+
+// Fallback for delay spreads too wide to stage: direct loads, one thread per
+// output sample (lanes along time keep the loads coalesced).
+template <typename T, bool SIGMA>
+__global__ void __launch_bounds__(256) k_dedisperse_direct(const DdKParams p) {
+  const long long t = (long long)blockIdx.x * 256 + threadIdx.x;
+  const int d = blockIdx.y;
+  const T* fb = reinterpret_cast<const T*>(p.fb);
+  float acc = 0.f, acc2 = 0.f;
+  int err = 0;
+  if (t < p.nt_out) {
+    for (int c = 0; c < p.nchan; ++c) {
+      const int o = __ldg(p.off + (long long)d * p.nchan + c);
+      if (t + o >= p.nrows_valid || o < 0) {
+        err |= kErrOffsetRange;
+        continue;
+      }
+      const unsigned long long rr = (unsigned long long)(p.row0 + t + o) & (unsigned long long)p.row_mask;
+      const float v = to_f<T>(fb[(long long)c * p.chan_stride + rr]);
+      if (sizeof(T) == 4) acc += v;
+      else acc = fmaf(p.chan_scale[c], v, acc);
+      if (SIGMA) acc2 = fmaf(v, v, acc2);
+    }
+    const float val = acc / (float)p.nchan;
+    p.out[(long long)d * p.out_stride + t] = val;
+    if (SIGMA) {
+      const double n = (double)p.nchan;
+      double var = ((double)acc2 - (double)acc * (double)acc / n) / (n * (n - 1.0));
+      p.sig_out[(long long)d * p.out_stride + t] = (float)sqrt(var > 0.0 ? var : 0.0);
+    }
+  }
+  // per-(DM, 256-sample block) partials
+  const float val = (t < p.nt_out) ? acc / (float)p.nchan : -INFINITY;
+  double s = (t < p.nt_out) ? (double)val : 0.0, s2 = s * s;
+  float mx = val;
+  int arg = (t < p.nt_out) ? (int)t : 0x7fffffff;
+  __shared__ double ss[8], ss2[8];
+  __shared__ float smx[8];
+  __shared__ int sarg[8];
+  s = wsum(s);
+  s2 = wsum(s2);
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    const float omx = __shfl_xor_sync(0xffffffffu, mx, o);
+    const int oarg = __shfl_xor_sync(0xffffffffu, arg, o);
+    if (omx > mx || (omx == mx && oarg < arg)) {
+      mx = omx;
+      arg = oarg;
+    }
+  }
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (lane == 0) {
+    ss[warp] = s;
+    ss2[warp] = s2;
+    smx[warp] = mx;
+    sarg[warp] = arg;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0 && p.part) {
+    DmPartial q{0.0, 0.0, -INFINITY, 0x7fffffff};
+    for (int w = 0; w < 8; ++w) {
+      q.s += ss[w];
+      q.s2 += ss2[w];
+      if (smx[w] > q.mx || (smx[w] == q.mx && sarg[w] < q.arg)) {
+        q.mx = smx[w];
+        q.arg = sarg[w];
+      }
+    }
+    p.part[(long long)blockIdx.x * p.ndm + d] = q;
+  }
+  if (err && p.err) atomicOr(p.err, err);
+}
+
+}  // namespace vfrb
+
+// ---- plan object --------------------------------------------------------------
+struct vfrb_ddplan {
+  int ndm = 0, nchan = 0;
+  int max_delay = 0;   // max over the table
+  int span16 = 0;      // max over 16-DM blocks and channels of (max - min) delay
+  int* d_off = nullptr;
+};
+
+namespace vfrb {
+
+static int dd_lmax(const vfrb_ddplan* pl, int vec) {
+  const int need = kDdNt + pl->span16 + vec;  // + alignment slack
+  return (need + 15) & ~15;
+}
+
+size_t dedisperse_workspace_bytes_plan(const vfrb_ddplan* pl, long long nt_out) {
+  const long long ntb = (nt_out + kDdNt - 1) / kDdNt;
+  return (size_t)ntb * (size_t)pl->ndm * sizeof(DmPartial);
+}
+
+template <typename T, bool SIGMA>
+static int dd_launch_t(const vfrb_ddplan* pl, const vfrb_dd_args& a, DdKParams& k, cudaStream_t s) {
+  constexpr int VEC = Vec<T>::n;
+  const int lmax = dd_lmax(pl, VEC);
+  const size_t fixed = ((size_t)kDdDm * kDdMaxChunk * 4 + kDdMaxChunk * 8 + kDdMaxChunk * 4 + 8 * 4 + 15) / 16 * 16;
+  int chunk = (int)((kDdSmemBudget - fixed) / ((size_t)lmax * sizeof(T)));
+  chunk = std::min(chunk, kDdMaxChunk);
+  const long long ntb = (a.nt_out + kDdNt - 1) / kDdNt;
+  const bool vec_ok = (a.chan_stride % VEC) == 0 && ((unsigned long long)a.row_mask + 1ULL) % VEC == 0;
+  if (chunk >= 4 && vec_ok) {
+    k.chunk = chunk;
+    k.lmax = lmax;
+    const size_t smem = ((size_t)kDdDm * chunk * 4 + chunk * 8 + chunk * 4 + 8 * 4 + 15) / 16 * 16 +
+                        (size_t)chunk * lmax * sizeof(T);
+    cudaError_t e = cudaFuncSetAttribute(k_dedisperse<T, SIGMA>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)smem);
+    if (e != cudaSuccess) return VFRB_ERR_CUDA;
+    dim3 grid((unsigned)ntb, (unsigned)((pl->ndm + kDdDm - 1) / kDdDm));
+    k_dedisperse<T, SIGMA><<<grid, kDdThreads, smem, s>>>(k);
+  } else {
+    dim3 grid((unsigned)ntb, (unsigned)pl->ndm);
+    k_dedisperse_direct<T, SIGMA><<<grid, 256, 0, s>>>(k);
+  }
+  return cuda_status(cudaGetLastError());
+}
+
+int launch_dedisperse_plan(const vfrb_ddplan* pl, const vfrb_dd_args& a, cudaStream_t s) {
+  if (!pl || !a.fb || !a.out) return VFRB_ERR_ARG;
+  if (a.nt_out <= 0) return a.nt_out == 0 ? VFRB_OK : VFRB_ERR_ARG;
+  if (a.nrows_valid < a.nt_out + pl->max_delay) return VFRB_ERR_ARG;
+  if (a.storage != VFRB_F32 && !a.chan_scale) return VFRB_ERR_ARG;
+  if (a.sigma_out && a.storage != VFRB_F32) return VFRB_ERR_UNSUPPORTED;
+  if ((unsigned long long)a.row_mask != 0xffffffffULL) {
+    const unsigned long long r = (unsigned long long)a.row_mask + 1ULL;
+    if ((r & (r - 1)) != 0) return VFRB_ERR_ARG;  // ring sizes are powers of two
+    if ((long long)r < a.nrows_valid) return VFRB_ERR_ARG;
+  }
+  const bool want_stats = a.ave || a.sigma || a.peak || a.frb || a.argmax;
+  const size_t ws = dedisperse_workspace_bytes_plan(pl, a.nt_out);
+  if (want_stats && (!a.workspace || a.workspace_bytes < ws)) return VFRB_ERR_ARG;
+  DdKParams k{};
+  k.fb = a.fb;
+  k.chan_scale = a.chan_scale;
+  k.chan_stride = a.chan_stride;
+  k.row0 = a.row0;
+  k.row_mask = a.row_mask;
+  k.nrows_valid = a.nrows_valid;
+  k.nchan = pl->nchan;
+  k.off = pl->d_off;
+  k.ndm = pl->ndm;
+  k.nt_out = a.nt_out;
+  k.out = a.out;
+  k.out_stride = a.out_stride;
+  k.sig_out = a.sigma_out;
+  k.part = want_stats ? reinterpret_cast<DmPartial*>(a.workspace) : nullptr;
+  k.err = a.d_err;
+  int st;
+  if (a.sigma_out) {
+    st = dd_launch_t<float, true>(pl, a, k, s);
+  } else {
+    switch (a.storage) {
+      case VFRB_F32: st = dd_launch_t<float, false>(pl, a, k, s); break;
+      case VFRB_F16: st = dd_launch_t<__half, false>(pl, a, k, s); break;
+      case VFRB_I8: st = dd_launch_t<int8_t, false>(pl, a, k, s); break;
+      default: return VFRB_ERR_ARG;
+    }
+  }
+  if (st || !want_stats) return st;
+  const long long ntb = (a.nt_out + kDdNt - 1) / kDdNt;
+  k_dm_stats<<<(pl->ndm + 7) / 8, 256, 0, s>>>(k.part, (int)ntb, pl->ndm, a.nt_out, a.ave, a.sigma, a.peak, a.frb,
+                                               a.argmax);
+  return cuda_status(cudaGetLastError());
+}
+
+int ddplan_create(vfrb_ddplan** out, const int32_t* h_off, int ndm, int nchan) {
+  if (!out || !h_off || ndm < 1 || nchan < 2) return VFRB_ERR_ARG;
+  vfrb_ddplan* p = new vfrb_ddplan();
+  p->ndm = ndm;
+  p->nchan = nchan;
+  int mxd = 0, span = 0;
+  for (long long i = 0; i < (long long)ndm * nchan; ++i) {
+    if (h_off[i] < 0) {
+      delete p;
+      return VFRB_ERR_ARG;
+    }
+    mxd = std::max(mxd, (int)h_off[i]);
+  }
+  for (int d0 = 0; d0 < ndm; d0 += kDdDm) {
+    for (int c = 0; c < nchan; ++c) {
+      int mn = 0x7fffffff, mx = 0;
+      for (int d = d0; d < std::min(ndm, d0 + kDdDm); ++d) {
+        mn = std::min(mn, (int)h_off[(long long)d * nchan + c]);
+        mx = std::max(mx, (int)h_off[(long long)d * nchan + c]);
+      }
+      span = std::max(span, mx - mn);
+    }
+  }
+  p->max_delay = mxd;
+  p->span16 = span;
+  const size_t bytes = sizeof(int) * (size_t)ndm * nchan;
+  if (cudaMalloc(&p->d_off, bytes) != cudaSuccess) {
+    delete p;
+    return VFRB_ERR_NOMEM;
+  }
+  if (cudaMemcpy(p->d_off, h_off, bytes, cudaMemcpyHostToDevice) != cudaSuccess) {
+    cudaFree(p->d_off);
+    delete p;
+    return VFRB_ERR_CUDA;
+  }
+  *out = p;
+  return VFRB_OK;
+}
+
+int ddplan_destroy(vfrb_ddplan* p) {
+  if (!p) return VFRB_OK;
+  if (p->d_off) cudaFree(p->d_off);
+  delete p;
+  return VFRB_OK;
+}
+
+}  // namespace vfrb
+
+namespace vfrb {
+int ddplan_max_delay(const vfrb_ddplan* p) { return p->max_delay; }
+}  // namespace vfrb

@@ -1,0 +1,33 @@
+// Shared definitions for the vlite-frb B200 kernels (sm_100a only).
+#pragma once
+#include <cuda_runtime.h>
+#include <cuda_fp16.h>
+#include <stdint.h>
+
+#include "../../include/vfrb.h"
+
+namespace vfrb {
+
+// VLITE VDIF geometry (PIPE:33-36).
+constexpr int kFrameLen = 5032;
+constexpr int kHdrLen = 32;
+constexpr int kDataLen = 5000;
+
+// The channeliser's transform length: TWONCHAN = 2*6250 (PIPE:1249).
+constexpr int kFftN = 12500;
+
+// Device-side error bits (the kernels never trap; they flag and skip).
+constexpr int kErrSlotRange = 1;     // sample position outside the slot table
+constexpr int kErrRowRange = 2;      // FB row outside the ring
+constexpr int kErrOffsetRange = 4;   // delay outside the prepared window
+
+inline int cuda_status(cudaError_t e) { return e == cudaSuccess ? VFRB_OK : VFRB_ERR_CUDA; }
+
+// Launchers (host side, defined in the .cu files).
+int launch_channelise(const vfrb_chan_args& a, cudaStream_t s);
+int launch_bandpass(const vfrb_bp_args& a, cudaStream_t s);
+int launch_chan_stats(const vfrb_cs_args& a, cudaStream_t s);
+int launch_fb_transpose(const float* src_cm, long long chan_stride, unsigned row_mask, long long row0,
+                        int nchan, int nrows, float* dst_tm, long long dst_row_stride, cudaStream_t s);
+
+}  // namespace vfrb
