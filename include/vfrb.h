@@ -147,6 +147,9 @@ typedef struct vfrb_ddplan vfrb_ddplan;
 int vfrb_ddplan_create(vfrb_ddplan** plan, const int32_t* h_offsets, int ndm, int nchan);
 int vfrb_ddplan_destroy(vfrb_ddplan* plan);
 int vfrb_ddplan_max_delay(const vfrb_ddplan* plan);
+/* Trials per register group of the fast kernel (4, 2 or 1), 0 when only the
+ * staged/direct kernels apply (no reference counterpart; introspection). */
+int vfrb_ddplan_group_size(const vfrb_ddplan* plan);
 
 typedef struct vfrb_dd_args {
   const void* fb;            /* device: channel-major FB in `storage` form       */
@@ -194,6 +197,125 @@ int vfrb_chan_stats(const vfrb_cs_args* a, void* stream);
  * PIPE:777). */
 int vfrb_fb_to_time_major(const float* src_cm, int64_t chan_stride, int64_t row0, uint32_t row_mask,
                           int nchan, int nrows, float* dst_tm, int64_t dst_row_stride, void* stream);
+
+/* ======================================================================
+ * Plan / stream API.  Replaces the main loops of the three tools
+ * (PIPE:556-708, STATS:367-431, TS:589-746): raw VDIF bytes go in as they
+ * arrive, results come out per block (reference semantics) or per chunk
+ * (streaming).  The drop-in tools and the serving loop are built on it.
+ * ====================================================================== */
+#define VFRB_PENDING 9             /* vfrb_poll: nothing ready yet        */
+
+#define VFRB_MODE_BLOCK 0          /* MAXTIME blocks, max_delay carry, block-relative
+                                      bandpass windows (PIPE:649-704, TS:643-692,
+                                      STATS:411-429)                       */
+#define VFRB_MODE_STREAM 1         /* continuous: absolute 128-row bandpass windows,
+                                      every output sample computed once    */
+
+#define VFRB_READER_PIPE 0         /* gaps = frame-number difference mod 25600 */
+#define VFRB_READER_TS 1           /* seconds-aware gaps (TS:895-937)      */
+
+#define VFRB_OUT_DEDISP 1          /* dedispersed series [ndm][nt]          */
+#define VFRB_OUT_DMSTATS 2         /* per-DM ave/sigma/peak/FRB/argmax      */
+#define VFRB_OUT_SIGMA 4           /* per-sample channel sigma (TS)         */
+#define VFRB_OUT_CHANSTATS 8       /* per-channel statistics (STATS)        */
+#define VFRB_OUT_FB 16             /* bandpass-subtracted FB, time-major    */
+#define VFRB_OUT_CANDS 32          /* candidate list                        */
+
+typedef struct vfrb_plan vfrb_plan;
+
+typedef struct vfrb_params {
+  int32_t twonchan, nave, nbundle; /* -nchan*2, -nave, -nb (PIPE:1245-1288)   */
+  double muoslowfreq;              /* 360 (default) or 384 (full band)       */
+  int32_t nchanout_fixed;          /* > 0 forces NCHANOUT (TS: 3840)         */
+  float maxtime;                   /* block length in seconds (MAXTIME)      */
+  float timestats;                 /* STATS statistics block (TIMESTATS)     */
+  const float* dms;                /* DM trial list (DM101.txt), host        */
+  int32_t ndm;
+  int32_t mode;                    /* VFRB_MODE_*                            */
+  int32_t reader;                  /* VFRB_READER_*                          */
+  int32_t dada_skip;               /* skip NFRAMEDADAINIT pairs first (TS)   */
+  int32_t storage;                 /* VFRB_F32 / VFRB_F16 / VFRB_I8          */
+  float q_scale;                   /* int8 quantisation (z units -> counts)  */
+  int32_t outputs;                 /* VFRB_OUT_* bits                        */
+  int32_t fb_block;                /* block whose FB is returned (-1: all)   */
+  int32_t nstreams;                /* independent streams (antennas)         */
+  float chunk_seconds;             /* streaming output chunk                 */
+  float ring_seconds;              /* device raw-frame ring per stream       */
+  float cand_snr;                  /* candidate threshold (peak SNR)         */
+  int32_t device;
+  int64_t device_bytes;            /* admission budget, 0 = 90% of free      */
+} vfrb_params;
+
+/* Reference defaults: 12500-point FFT, NAVE 4, NBUNDLE 32, 3908 channels,
+ * MAXTIME 70 s, block mode, FP32, one stream. */
+void vfrb_params_default(vfrb_params* p);
+
+typedef struct vfrb_cand {
+  int32_t dm_index;
+  int32_t width;                   /* boxcar width in samples (1 = none)     */
+  int64_t t;                       /* absolute FB row of the peak            */
+  float snr;
+  float dm;
+} vfrb_cand;
+
+typedef struct vfrb_result {
+  int32_t stream;
+  int64_t seq;                     /* block (block mode) or chunk index      */
+  int64_t row0;                    /* absolute FB row of output sample 0     */
+  double tstart_mjd;               /* getVDIFDMJD of the first frame used    */
+  int32_t ndm;
+  int64_t nt;
+  const float* dd;                 /* [ndm][nt] or NULL                      */
+  const float* dd_sigma;           /* [ndm][nt] or NULL                      */
+  const float* ave;                /* [ndm] each, or NULL                    */
+  const float* sigma;
+  const float* peak;
+  const int32_t* frb;
+  const int32_t* argmax;
+  int32_t nchan;
+  int64_t fb_rows;
+  const float* fb;                 /* [fb_rows][nchan] or NULL               */
+  int32_t nstatblks;
+  const float* chan_ave;           /* [nstatblks][nchan] each, or NULL       */
+  const float* chan_sig;
+  const float* chan_outlier;
+  int32_t ncand;
+  const vfrb_cand* cands;
+  double latency_ms;               /* data complete -> result on the host    */
+  int32_t device_errors;           /* kernel error bits seen (0 = none)      */
+} vfrb_result;
+
+int vfrb_plan_create(vfrb_plan** plan, const vfrb_params* params);
+int vfrb_plan_destroy(vfrb_plan* plan);
+/* Derived layout and the max_delay in FB rows used for the overlap carry. */
+int vfrb_plan_layout(const vfrb_plan* plan, vfrb_layout* L, int32_t* max_delay);
+int64_t vfrb_plan_device_bytes(const vfrb_plan* plan);
+
+/* Feed raw VDIF bytes of one stream (any split; frames may straddle calls).
+ * nbytes == 0 marks end of data (the reference's EOF/EOD).  Page-locked
+ * input is copied to the device directly, other input through a staging
+ * buffer; `bytes` may be reused as soon as the call returns. */
+int vfrb_push_frames(vfrb_plan* plan, int stream, const uint8_t* bytes, size_t nbytes);
+
+/* Next completed result in submission order.  Returns VFRB_OK with *out
+ * filled (host buffers owned by the plan, valid until the next poll),
+ * VFRB_PENDING when work is in flight but not done (wait == 0), or
+ * VFRB_EOD when every stream has ended and nothing is left. */
+int vfrb_poll(vfrb_plan* plan, vfrb_result* out, int wait);
+
+/* Host-only: run the pol-pair reader of the plan API over a byte buffer fed
+ * in pieces of `split` bytes (0 = one piece), as initframe01 +
+ * readtwoframe (PIPE:1031-1131; TS:767-1145 with reader VFRB_READER_TS).
+ * Writes the pair sequence as frame indices into the input (-1 = zero fill
+ * frame); entry 0 is the pair initframe01 leaves in the buffers.  Returns
+ * VFRB_OK, or VFRB_ERR when initialisation fails (the reference exits 2). */
+int vfrb_read_pairs(const uint8_t* bytes, size_t nbytes, int reader_mode, int dada_skip, size_t split,
+                    int64_t* e0, int64_t* e1, int64_t cap, int64_t* npairs, double* tstart_mjd);
+
+/* Reader log lines (frame skips, misalignment) of a stream, '\n'-joined;
+ * valid until the next call.  Mirrors the reference's <OUT>.log messages. */
+const char* vfrb_stream_log(vfrb_plan* plan, int stream);
 
 #ifdef __cplusplus
 }

@@ -100,6 +100,7 @@ for _n, _t in (("vfrb_channelise", ChanArgs), ("vfrb_bandpass", BpArgs), ("vfrb_
 _lib.vfrb_ddplan_create.argtypes = [C.POINTER(C.c_void_p), C.c_void_p, C.c_int, C.c_int]
 _lib.vfrb_ddplan_destroy.argtypes = [C.c_void_p]
 _lib.vfrb_ddplan_max_delay.argtypes = [C.c_void_p]
+_lib.vfrb_ddplan_group_size.argtypes = [C.c_void_p]
 _lib.vfrb_dedisperse_workspace_bytes.restype = C.c_size_t
 _lib.vfrb_dedisperse_workspace_bytes.argtypes = [C.c_void_p, C.c_int64]
 _lib.vfrb_dedisperse.argtypes = [C.c_void_p, C.POINTER(DdArgs), C.c_void_p]
@@ -208,6 +209,7 @@ class DedispPlan:
         _check(_lib.vfrb_ddplan_create(C.byref(p), off.ctypes.data, self.ndm, self.nchan), "vfrb_ddplan_create")
         self._p = p
         self.max_delay = _lib.vfrb_ddplan_max_delay(p)
+        self.group_size = _lib.vfrb_ddplan_group_size(p)
 
     def workspace_bytes(self, nt_out: int) -> int:
         return int(_lib.vfrb_dedisperse_workspace_bytes(self._p, nt_out))

@@ -16,6 +16,8 @@
 #include "vfrb_common.cuh"
 
 #include <algorithm>
+#include <cstdint>
+#include <cstdlib>
 #include <vector>
 
 namespace vfrb {
@@ -345,12 +347,19 @@ __global__ void __launch_bounds__(256) k_dedisperse_direct(const DdKParams p) {
 
 }  // namespace vfrb
 
+#include "dedisperse_reg.cuh"
+
 // ---- plan object --------------------------------------------------------------
 struct vfrb_ddplan {
   int ndm = 0, nchan = 0;
   int max_delay = 0;   // max over the table
   int span16 = 0;      // max over 16-DM blocks and channels of (max - min) delay
   int* d_off = nullptr;
+  // register-window variant: groups of D adjacent trials, shifts <= smax
+  int reg_d = 0, reg_smax = 0, reg_span = 0, ngroups = 0, nblocks = 0;
+  int* d_gbase = nullptr;
+  unsigned* d_gpack = nullptr;
+  int* d_bmin = nullptr;
 };
 
 namespace vfrb {
@@ -391,6 +400,68 @@ static int dd_launch_t(const vfrb_ddplan* pl, const vfrb_dd_args& a, DdKParams& 
   return cuda_status(cudaGetLastError());
 }
 
+template <typename T, int D, int TT, int SMAX>
+static int reg_launch_t(const vfrb_ddplan* pl, const vfrb_dd_args& a, DmPartial* part, cudaStream_t s, int* ntb) {
+  using Cfg = RegCfg<T, D, TT, SMAX>;
+  const int lmax = (Cfg::NT + pl->reg_span + Cfg::VEC + Cfg::NW + 15) & ~15;
+  const int per_ch = lmax * (int)sizeof(T) * 2 + 2 * (2 * kRegWarps * 4 + 8);
+  int chunk = std::min(32, (int)(96 * 1024 / per_ch));
+  *ntb = 0;
+  if (chunk < 2) return VFRB_OK;  // caller falls back (ntb == 0)
+  DdRegParams k{};
+  k.fb = a.fb;
+  k.chan_scale = a.chan_scale;
+  k.chan_stride = a.chan_stride;
+  k.row0 = a.row0;
+  k.row_mask = a.row_mask;
+  k.nrows_valid = a.nrows_valid;
+  k.nchan = pl->nchan;
+  k.ndm = pl->ndm;
+  k.ngroups = pl->ngroups;
+  k.nt_out = a.nt_out;
+  k.out = a.out;
+  k.out_stride = a.out_stride;
+  k.part = part;
+  k.gbase = pl->d_gbase;
+  k.gpack = pl->d_gpack;
+  k.bmin = pl->d_bmin;
+  k.chunk = chunk;
+  k.lmax = lmax;
+  k.err = a.d_err;
+  const int meta_words = 2 * kRegWarps * chunk + 2 * chunk;
+  const size_t smem = (size_t)(2 * meta_words * 4 + 15) / 16 * 16 + (size_t)2 * chunk * lmax * sizeof(T);
+  cudaError_t e = cudaFuncSetAttribute(k_dedisp_reg<T, D, TT, SMAX>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)smem);
+  if (e != cudaSuccess) return VFRB_ERR_CUDA;
+  dim3 grid((unsigned)((a.nt_out + Cfg::NT - 1) / Cfg::NT), (unsigned)pl->nblocks);
+  k_dedisp_reg<T, D, TT, SMAX><<<grid, kRegWarps * 32, smem, s>>>(k);
+  const int st = cuda_status(cudaGetLastError());
+  if (st == VFRB_OK) *ntb = (int)grid.x;  // time blocks, for the statistics reduction
+  return st;
+}
+
+// Launches the register-window kernel when it applies.  Returns a status;
+// *ntb is the number of time blocks launched, 0 when the variant does not
+// apply (the caller then uses the staged or direct kernel).
+static int reg_launch(const vfrb_ddplan* pl, const vfrb_dd_args& a, DmPartial* part, cudaStream_t s, int* ntb) {
+  *ntb = 0;
+  if (pl->reg_d == 0) return VFRB_OK;
+  if (((uintptr_t)a.fb & 15) != 0) return VFRB_OK;
+  if (a.storage == VFRB_F32) {
+    if (a.chan_stride % 4 || ((unsigned long long)a.row_mask + 1ULL) % 4) return VFRB_OK;
+    if (pl->reg_d == 4) return reg_launch_t<float, 4, 15, 20>(pl, a, part, s, ntb);
+    if (pl->reg_d == 2) return reg_launch_t<float, 2, 15, 16>(pl, a, part, s, ntb);
+    return reg_launch_t<float, 1, 15, 0>(pl, a, part, s, ntb);
+  }
+  if (a.storage == VFRB_F16) {
+    if (a.chan_stride % 8 || ((unsigned long long)a.row_mask + 1ULL) % 8) return VFRB_OK;
+    if (pl->reg_d == 4) return reg_launch_t<__half, 4, 14, 20>(pl, a, part, s, ntb);
+    if (pl->reg_d == 2) return reg_launch_t<__half, 2, 14, 16>(pl, a, part, s, ntb);
+    return reg_launch_t<__half, 1, 14, 0>(pl, a, part, s, ntb);
+  }
+  return VFRB_OK;
+}
+
 int launch_dedisperse_plan(const vfrb_ddplan* pl, const vfrb_dd_args& a, cudaStream_t s) {
   if (!pl || !a.fb || !a.out) return VFRB_ERR_ARG;
   if (a.nt_out <= 0) return a.nt_out == 0 ? VFRB_OK : VFRB_ERR_ARG;
@@ -422,6 +493,17 @@ int launch_dedisperse_plan(const vfrb_ddplan* pl, const vfrb_dd_args& a, cudaStr
   k.part = want_stats ? reinterpret_cast<DmPartial*>(a.workspace) : nullptr;
   k.err = a.d_err;
   int st;
+  if (!a.sigma_out && !getenv("VFRB_DD_V1")) {
+    int ntb = 0;
+    const int rst = reg_launch(pl, a, k.part, s, &ntb);
+    if (rst) return rst;
+    if (ntb > 0) {
+      if (!want_stats) return VFRB_OK;
+      k_dm_stats<<<(pl->ndm + 7) / 8, 256, 0, s>>>(k.part, ntb, pl->ndm, a.nt_out, a.ave, a.sigma, a.peak, a.frb,
+                                                   a.argmax);
+      return cuda_status(cudaGetLastError());
+    }
+  }
   if (a.sigma_out) {
     st = dd_launch_t<float, true>(pl, a, k, s);
   } else {
@@ -464,6 +546,66 @@ int ddplan_create(vfrb_ddplan** out, const int32_t* h_off, int ndm, int nchan) {
   }
   p->max_delay = mxd;
   p->span16 = span;
+  // register-window grouping: the largest D in {4, 2, 1} whose in-group shifts fit the kernel
+  for (int D : {4, 2, 1}) {
+    const int smax_allowed = (D == 4) ? 20 : (D == 2) ? 16 : 0;
+    const int ng = (ndm + D - 1) / D;
+    int need = 0;
+    for (int g = 0; g < ng && need <= smax_allowed; ++g)
+      for (int c = 0; c < nchan; ++c) {
+        int mn = 0x7fffffff, mx = 0;
+        for (int j = 0; j < D; ++j) {
+          const int d = std::min(g * D + j, ndm - 1);
+          mn = std::min(mn, (int)h_off[(long long)d * nchan + c]);
+          mx = std::max(mx, (int)h_off[(long long)d * nchan + c]);
+        }
+        need = std::max(need, mx - mn);
+      }
+    if (need > smax_allowed) continue;
+    const int DB = kRegWarps * D;
+    p->reg_d = D;
+    p->reg_smax = smax_allowed;
+    p->ngroups = ng;
+    p->nblocks = (ndm + DB - 1) / DB;
+    std::vector<int> gb((size_t)ng * nchan), bm((size_t)p->nblocks * nchan);
+    std::vector<unsigned> gp((size_t)ng * nchan);
+    int rspan = 0;
+    for (int g = 0; g < ng; ++g)
+      for (int c = 0; c < nchan; ++c) {
+        int mn = 0x7fffffff;
+        for (int j = 0; j < D; ++j) mn = std::min(mn, (int)h_off[(long long)std::min(g * D + j, ndm - 1) * nchan + c]);
+        unsigned pk = 0;
+        for (int j = 0; j < D; ++j)
+          pk |= (unsigned)(h_off[(long long)std::min(g * D + j, ndm - 1) * nchan + c] - mn) << (8 * j);
+        gb[(size_t)g * nchan + c] = mn;
+        gp[(size_t)g * nchan + c] = pk;
+      }
+    for (int b = 0; b < p->nblocks; ++b)
+      for (int c = 0; c < nchan; ++c) {
+        int mn = 0x7fffffff, mx = 0;
+        for (int d = b * DB; d < std::min(ndm, (b + 1) * DB); ++d) {
+          mn = std::min(mn, (int)h_off[(long long)d * nchan + c]);
+          mx = std::max(mx, (int)h_off[(long long)d * nchan + c]);
+        }
+        bm[(size_t)b * nchan + c] = mn;
+        rspan = std::max(rspan, mx - mn);
+      }
+    p->reg_span = rspan;
+    bool ok = cudaMalloc(&p->d_gbase, gb.size() * sizeof(int)) == cudaSuccess &&
+              cudaMalloc(&p->d_gpack, gp.size() * sizeof(unsigned)) == cudaSuccess &&
+              cudaMalloc(&p->d_bmin, bm.size() * sizeof(int)) == cudaSuccess;
+    ok = ok && cudaMemcpy(p->d_gbase, gb.data(), gb.size() * sizeof(int), cudaMemcpyHostToDevice) == cudaSuccess &&
+         cudaMemcpy(p->d_gpack, gp.data(), gp.size() * sizeof(unsigned), cudaMemcpyHostToDevice) == cudaSuccess &&
+         cudaMemcpy(p->d_bmin, bm.data(), bm.size() * sizeof(int), cudaMemcpyHostToDevice) == cudaSuccess;
+    if (!ok) {
+      cudaFree(p->d_gbase);
+      cudaFree(p->d_gpack);
+      cudaFree(p->d_bmin);
+      delete p;
+      return VFRB_ERR_NOMEM;
+    }
+    break;
+  }
   const size_t bytes = sizeof(int) * (size_t)ndm * nchan;
   if (cudaMalloc(&p->d_off, bytes) != cudaSuccess) {
     delete p;
@@ -481,6 +623,9 @@ int ddplan_create(vfrb_ddplan** out, const int32_t* h_off, int ndm, int nchan) {
 int ddplan_destroy(vfrb_ddplan* p) {
   if (!p) return VFRB_OK;
   if (p->d_off) cudaFree(p->d_off);
+  if (p->d_gbase) cudaFree(p->d_gbase);
+  if (p->d_gpack) cudaFree(p->d_gpack);
+  if (p->d_bmin) cudaFree(p->d_bmin);
   delete p;
   return VFRB_OK;
 }
@@ -489,4 +634,5 @@ int ddplan_destroy(vfrb_ddplan* p) {
 
 namespace vfrb {
 int ddplan_max_delay(const vfrb_ddplan* p) { return p->max_delay; }
+int ddplan_reg_group(const vfrb_ddplan* p) { return p->reg_d; }
 }  // namespace vfrb

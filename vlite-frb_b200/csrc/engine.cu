@@ -1,0 +1,964 @@
+// Plan / stream engine behind vfrb_plan_* (the reference's main loops,
+// PIPE:556-708, STATS:367-431, TS:589-746), B200 style:
+//
+//  * raw VDIF bytes are copied once to a per-stream device frame ring on a
+//    copy stream; only headers are parsed on the host, by the reference's
+//    pol-pair state machine (vdif_reader.h), which emits payload references;
+//  * complete rows are channelised straight from the ring (K1), bandpassed
+//    into the layout/precision the dedisperser wants (K2), dedispersed with
+//    fused statistics (K3) or reduced to per-channel statistics (K4), all on
+//    the stream's compute stream, overlapping the next copy;
+//  * results are copied to page-locked host memory and handed out by
+//    vfrb_poll() as they complete; a host callback stamps completion time
+//    for latency accounting.
+//
+// Block mode reproduces the reference's block manager: a MAXNT-row
+// filterbank filled NBUNDLE rows at a time, the raw last max_delay rows
+// carried to the next block with new data written from row
+// (max_delay/NBUNDLE)*NBUNDLE (PIPE:649-704; TS:643-692), bandpass windows
+// counted from the block's first row; STATS restarts at row 0 (STATS:428).
+// Stream mode keeps a max_delay overlap ring per stream, bandpasses absolute
+// 128-row windows and emits every output sample once.
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <deque>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "vdif_reader.h"
+#include "vfrb_common.cuh"
+
+namespace vfrb {
+size_t dedisperse_workspace_bytes_plan(const vfrb_ddplan* pl, long long nt_out);
+int launch_dedisperse_plan(const vfrb_ddplan* pl, const vfrb_dd_args& a, cudaStream_t s);
+int ddplan_create(vfrb_ddplan** out, const int32_t* h_off, int ndm, int nchan);
+int ddplan_destroy(vfrb_ddplan* p);
+int ddplan_max_delay(const vfrb_ddplan* p);
+
+static double now_ms() {
+  using namespace std::chrono;
+  return duration<double, std::milli>(steady_clock::now().time_since_epoch()).count();
+}
+
+#define CK(x)                                     \
+  do {                                            \
+    if ((x) != cudaSuccess) {                     \
+      cudaGetLastError();                         \
+      return VFRB_ERR_CUDA;                       \
+    }                                             \
+  } while (0)
+#define ST(x)            \
+  do {                   \
+    const int st_ = (x); \
+    if (st_) return st_; \
+  } while (0)
+
+constexpr int kStash = 1024;   // gap-revealing frames kept aside per stream
+constexpr int kSlotBufs = 4;   // rotating slot-table uploads in flight
+constexpr int kStageBufs = 2;  // rotating staging buffers for pageable input
+
+static unsigned long long pow2_at_least(unsigned long long v) {
+  unsigned long long r = 1;
+  while (r < v) r <<= 1;
+  return r;
+}
+
+// Per-channel weights of the FP16 / int8 forms from the first bandpass
+// window's variance: s_c = sqrt(var_c); stored z = x/s_c (times q for int8);
+// the dedisperser weights channel c by s_c (s_c/q for int8).
+__global__ void k_init_scale(const float* var, int nchan, float q, int storage, float* w, float* inv) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= nchan) return;
+  float s = sqrtf(fmaxf(var[c], 0.f));
+  if (!(s > 1e-30f)) s = 1.f;
+  inv[c] = 1.f / s;
+  w[c] = (storage == VFRB_I8) ? s / q : s;
+}
+
+struct ResultSlot {
+  vfrb_result r{};
+  float *dd = nullptr, *dds = nullptr, *ave = nullptr, *sig = nullptr, *peak = nullptr, *fb = nullptr;
+  int32_t *frb = nullptr, *arg = nullptr, *err = nullptr;
+  float *cave = nullptr, *csig = nullptr, *cout = nullptr;
+  std::vector<vfrb_cand> cands;
+  cudaEvent_t ev = nullptr;
+  double t_data = 0.0;
+  volatile double t_done = 0.0;
+  int state = 0;  // 0 free, 1 in flight, 2 held by the caller
+};
+
+static void CUDART_CB mark_done(void* p) { static_cast<ResultSlot*>(p)->t_done = now_ms(); }
+
+struct SlotBuf {
+  int64_t* h = nullptr;
+  int64_t* d = nullptr;
+  cudaEvent_t ev = nullptr;
+};
+
+struct StreamSt {
+  int id = 0;
+  cudaStream_t cs = nullptr;   // compute
+  cudaStream_t xs = nullptr;   // host-to-device copies
+  cudaEvent_t ev_copied = nullptr, ev_consumed = nullptr;
+  std::unique_ptr<PairReader> reader;
+  std::vector<uint8_t> part;   // bytes of an incomplete frame
+  uint8_t* d_frames = nullptr; // frame ring followed by the stash
+  int64_t ring_frames = 0;
+  int64_t frames_in = 0;       // frames received (ring position)
+  int stash_next = 0;
+  uint8_t* h_stage[kStageBufs] = {};
+  cudaEvent_t stage_ev[kStageBufs] = {};
+  int stage_i = 0;
+  size_t stage_frames = 0;
+  SlotBuf sb[kSlotBufs];
+  int sb_i = 0;
+  int64_t slots_cap = 0;
+  std::vector<int64_t> e0, e1;  // pair entries: frame index, -1 fill, <= -2 stash slot
+  size_t ehead = 0;             // consumed entries at the front of e0/e1
+  int64_t ebase = 0;            // global index of e0[ehead]
+  bool ended = false;
+  bool started = false;
+  int reader_error = 0;
+  double tstart_mjd = 0.0;
+  std::string logtext;
+  double t_push = 0.0;
+  int32_t* d_err = nullptr;
+  // block mode
+  float* d_fb_tm = nullptr;
+  float* d_left = nullptr;
+  int64_t bundles_done = 0;
+  int loopcnt = 0;
+  int64_t blocks = 0;
+  // stream mode
+  float* d_raw = nullptr;
+  int64_t R1 = 0;
+  int64_t rows_chan = 0, rows_bp = 0, rows_out = 0;
+  int64_t chunks = 0;
+  // both
+  void* d_cm = nullptr;  // channel-major bandpassed FB (storage form)
+  int64_t cm_stride = 0;
+  unsigned cm_mask = 0xffffffffu;
+  float *d_w = nullptr, *d_inv = nullptr, *d_var = nullptr, *d_scr = nullptr;
+  bool scale_ready = false;
+  float *d_out = nullptr, *d_sig = nullptr, *d_ave = nullptr, *d_sgm = nullptr, *d_peak = nullptr;
+  int32_t *d_frb = nullptr, *d_arg = nullptr;
+  void* d_ws = nullptr;
+  size_t ws_bytes = 0;
+  float *d_cave = nullptr, *d_csig = nullptr, *d_cout = nullptr, *d_fbt = nullptr;
+  int64_t out_stride = 0;
+  std::vector<std::unique_ptr<ResultSlot>> slots;
+};
+
+}  // namespace vfrb
+
+using namespace vfrb;
+
+struct vfrb_plan {
+  vfrb_params P{};
+  vfrb_layout L{};
+  std::vector<float> dms;
+  std::vector<int32_t> off;
+  int max_delay = 0;
+  int ndm = 0;
+  vfrb_ddplan* dd = nullptr;
+  bool want_dd = false;
+  int64_t chunk_rows = 0;
+  int64_t nt_block = 0;
+  int64_t launch_rows = 0;  // most rows one channelise launch produces
+  int ncolstatblk = 0, nstatblks = 0;
+  int64_t dev_bytes = 0;
+  std::vector<std::unique_ptr<StreamSt>> st;
+  std::deque<ResultSlot*> queue;  // submission order
+  ResultSlot* held = nullptr;     // returned by the last poll
+  std::string logtmp;
+  std::vector<void*> dev_allocs, host_allocs;
+  std::vector<cudaEvent_t> events;
+  std::vector<cudaStream_t> streams;
+};
+
+namespace {
+
+bool is_pinned(const void* p) {
+  cudaPointerAttributes a{};
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return a.type == cudaMemoryTypeHost;
+}
+
+template <typename T>
+int dmalloc(vfrb_plan* pl, T** p, size_t bytes) {
+  if (bytes == 0) bytes = 16;
+  if (cudaMalloc((void**)p, bytes) != cudaSuccess) {
+    cudaGetLastError();
+    *p = nullptr;
+    return VFRB_ERR_NOMEM;
+  }
+  pl->dev_allocs.push_back((void*)*p);
+  pl->dev_bytes += (int64_t)bytes;
+  return VFRB_OK;
+}
+
+template <typename T>
+int hmalloc(vfrb_plan* pl, T** p, size_t bytes) {
+  if (bytes == 0) bytes = 16;
+  if (cudaHostAlloc((void**)p, bytes, cudaHostAllocDefault) != cudaSuccess) {
+    cudaGetLastError();
+    *p = nullptr;
+    return VFRB_ERR_NOMEM;
+  }
+  pl->host_allocs.push_back((void*)*p);
+  return VFRB_OK;
+}
+
+int mkevent(vfrb_plan* pl, cudaEvent_t* e) {
+  CK(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
+  pl->events.push_back(*e);
+  return VFRB_OK;
+}
+
+size_t storage_bytes(int s) { return s == VFRB_F32 ? 4 : (s == VFRB_F16 ? 2 : 1); }
+
+bool want(const vfrb_plan* pl, int bit) { return (pl->P.outputs & bit) != 0; }
+
+// device bytes one stream needs (admission control)
+int64_t stream_bytes(const vfrb_plan* pl, int64_t ring_frames, int64_t R1, int64_t R2) {
+  const vfrb_params& P = pl->P;
+  const int64_t nch = pl->L.nchanout;
+  int64_t b = ring_frames * kFrameLen + (int64_t)kStash * kDataLen + kSlotBufs * 2 * 16 * pl->launch_rows * 64;
+  const int64_t nt = P.mode == VFRB_MODE_BLOCK ? pl->nt_block : pl->chunk_rows;
+  if (P.mode == VFRB_MODE_BLOCK) {
+    b += (int64_t)pl->L.maxnt * nch * 4;                                    // raw block
+    b += (int64_t)pl->max_delay * nch * 4;                                  // leftover
+    b += nch * (((int64_t)pl->L.maxnt + 15) / 16 * 16) * (int64_t)storage_bytes(P.storage);
+    if (want(pl, VFRB_OUT_FB)) b += (int64_t)pl->L.maxnt * nch * 4;
+    if (want(pl, VFRB_OUT_CHANSTATS)) b += 3LL * pl->nstatblks * nch * 4;
+  } else {
+    b += R1 * nch * 4 + R2 * nch * (int64_t)storage_bytes(P.storage);
+  }
+  if (pl->want_dd) {
+    b += (int64_t)pl->ndm * nt * 4 * (want(pl, VFRB_OUT_SIGMA) ? 2 : 1);
+    b += (int64_t)dedisperse_workspace_bytes_plan(pl->dd, nt) + 5LL * pl->ndm * 4;
+  }
+  return b;
+}
+
+int alloc_slot(vfrb_plan* pl, StreamSt* s, ResultSlot** out) {
+  for (auto& r : s->slots)
+    if (r->state == 0) {
+      *out = r.get();
+      return VFRB_OK;
+    }
+  auto r = std::make_unique<ResultSlot>();
+  const vfrb_params& P = pl->P;
+  const int64_t nch = pl->L.nchanout;
+  const int64_t nt = P.mode == VFRB_MODE_BLOCK ? pl->nt_block : pl->chunk_rows;
+  if (pl->want_dd) {
+    if (want(pl, VFRB_OUT_DEDISP)) ST(hmalloc(pl, &r->dd, (size_t)pl->ndm * nt * 4));
+    if (want(pl, VFRB_OUT_SIGMA)) ST(hmalloc(pl, &r->dds, (size_t)pl->ndm * nt * 4));
+    ST(hmalloc(pl, &r->ave, (size_t)pl->ndm * 4));
+    ST(hmalloc(pl, &r->sig, (size_t)pl->ndm * 4));
+    ST(hmalloc(pl, &r->peak, (size_t)pl->ndm * 4));
+    ST(hmalloc(pl, &r->frb, (size_t)pl->ndm * 4));
+    ST(hmalloc(pl, &r->arg, (size_t)pl->ndm * 4));
+  }
+  if (P.mode == VFRB_MODE_BLOCK && want(pl, VFRB_OUT_FB)) ST(hmalloc(pl, &r->fb, (size_t)pl->L.maxnt * nch * 4));
+  if (P.mode == VFRB_MODE_BLOCK && want(pl, VFRB_OUT_CHANSTATS)) {
+    ST(hmalloc(pl, &r->cave, (size_t)pl->nstatblks * nch * 4));
+    ST(hmalloc(pl, &r->csig, (size_t)pl->nstatblks * nch * 4));
+    ST(hmalloc(pl, &r->cout, (size_t)pl->nstatblks * nch * 4));
+  }
+  ST(hmalloc(pl, &r->err, 4));
+  ST(mkevent(pl, &r->ev));
+  *out = r.get();
+  s->slots.push_back(std::move(r));
+  return VFRB_OK;
+}
+
+// Translate a pair entry into a payload byte offset within d_frames.
+inline int64_t entry_offset(const StreamSt* s, int64_t v) {
+  if (v >= 0) return (v % s->ring_frames) * kFrameLen + kHdrLen;
+  if (v == -1) return -1;
+  return s->ring_frames * kFrameLen + (-2 - v) * (int64_t)kDataLen;
+}
+
+int64_t npairs(const StreamSt* s) { return s->ebase + (int64_t)(s->e0.size() - s->ehead); }
+
+void consume_entries(StreamSt* s, int64_t first_needed) {
+  while (s->ebase < first_needed && s->ehead < s->e0.size()) {
+    ++s->ehead;
+    ++s->ebase;
+  }
+  if (s->ehead > 65536 && s->ehead * 2 > s->e0.size()) {
+    s->e0.erase(s->e0.begin(), s->e0.begin() + (long)s->ehead);
+    s->e1.erase(s->e1.begin(), s->e1.begin() + (long)s->ehead);
+    s->ehead = 0;
+  }
+}
+
+// Channelise `nrows` FB rows starting at stream row `row_first` into `out`
+// (ring row out_row0, mask).  Samples of row r are stream positions
+// [r*S, (r+1)*S) of each pol, S = NAVE*TWONCHAN.
+int launch_rows(vfrb_plan* pl, StreamSt* s, int64_t row_first, int64_t nrows, float* out, int64_t out_row0,
+                unsigned mask) {
+  const vfrb_layout& L = pl->L;
+  const int64_t S = (int64_t)L.nave * L.twonchan;
+  const int64_t p0 = row_first * S, p1 = (row_first + nrows) * S;
+  const int64_t e_lo = p0 / kDataLen, e_hi = (p1 + kDataLen - 1) / kDataLen;
+  const int64_t n = e_hi - e_lo;
+  if (n > s->slots_cap || e_lo < s->ebase || e_hi > npairs(s)) return VFRB_ERR;
+  SlotBuf& b = s->sb[s->sb_i];
+  s->sb_i = (s->sb_i + 1) % kSlotBufs;
+  CK(cudaEventSynchronize(b.ev));  // the upload from this buffer four launches ago is done
+  for (int64_t i = 0; i < n; ++i) {
+    const size_t k = s->ehead + (size_t)(e_lo - s->ebase + i);
+    b.h[i] = entry_offset(s, s->e0[k]);
+    b.h[s->slots_cap + i] = entry_offset(s, s->e1[k]);
+  }
+  CK(cudaMemcpyAsync(b.d, b.h, sizeof(int64_t) * n, cudaMemcpyHostToDevice, s->cs));
+  CK(cudaMemcpyAsync(b.d + s->slots_cap, b.h + s->slots_cap, sizeof(int64_t) * n, cudaMemcpyHostToDevice, s->cs));
+  CK(cudaEventRecord(b.ev, s->cs));
+  vfrb_chan_args a{};
+  a.frames = s->d_frames;
+  a.slots0 = b.d;
+  a.slots1 = b.d + s->slots_cap;
+  a.nslots = n;
+  a.sample0 = p0 - e_lo * kDataLen;
+  a.nrows = (int32_t)nrows;
+  a.twonchan = L.twonchan;
+  a.nave = L.nave;
+  a.nfreq = L.nfreq;
+  a.nskip = L.nskip;
+  a.nchanout = L.nchanout;
+  a.out = out;
+  a.out_row_stride = L.nchanout;
+  a.out_row0 = out_row0;
+  a.out_row_mask = mask;
+  a.d_err = s->d_err;
+  ST(launch_channelise(a, s->cs));
+  CK(cudaEventRecord(s->ev_consumed, s->cs));
+  return VFRB_OK;
+}
+
+// FP16/int8: weights from the variance of the first window (one extra F32
+// bandpass pass of 128 rows into scratch).
+int init_scale(vfrb_plan* pl, StreamSt* s, const float* raw, int64_t row0, unsigned mask) {
+  if (s->scale_ready || pl->P.storage == VFRB_F32) return VFRB_OK;
+  vfrb_bp_args a{};
+  a.in = raw;
+  a.in_row_stride = pl->L.nchanout;
+  a.in_row0 = row0;
+  a.in_row_mask = mask;
+  a.nchan = pl->L.nchanout;
+  a.nrows = 128;
+  a.window = 128;
+  a.storage = VFRB_F32;
+  a.out = s->d_scr;
+  a.out_chan_stride = 128;
+  a.out_row_mask = 0xffffffffu;
+  a.win_var = s->d_var;
+  ST(launch_bandpass(a, s->cs));
+  const int nch = pl->L.nchanout;
+  k_init_scale<<<(nch + 255) / 256, 256, 0, s->cs>>>(s->d_var, nch, pl->P.q_scale, pl->P.storage, s->d_w, s->d_inv);
+  CK(cudaGetLastError());
+  s->scale_ready = true;
+  return VFRB_OK;
+}
+
+int run_bandpass(vfrb_plan* pl, StreamSt* s, const float* raw, int64_t in_row0, unsigned in_mask, int64_t nrows,
+                 int64_t out_row0, float* tm_out) {
+  ST(init_scale(pl, s, raw, in_row0, in_mask));
+  vfrb_bp_args a{};
+  a.in = raw;
+  a.in_row_stride = pl->L.nchanout;
+  a.in_row0 = in_row0;
+  a.in_row_mask = in_mask;
+  a.nchan = pl->L.nchanout;
+  a.nrows = (int32_t)nrows;
+  a.window = 128;
+  a.storage = pl->P.storage;
+  a.out = s->d_cm;
+  a.out_chan_stride = s->cm_stride;
+  a.out_row0 = out_row0;
+  a.out_row_mask = s->cm_mask;
+  a.inv_scale = pl->P.storage == VFRB_F32 ? nullptr : s->d_inv;
+  a.q_scale = pl->P.q_scale;
+  a.tm_out = tm_out;
+  a.tm_row_stride = pl->L.nchanout;
+  a.d_err = s->d_err;
+  return launch_bandpass(a, s->cs);
+}
+
+int run_dedisp(vfrb_plan* pl, StreamSt* s, int64_t row0, int64_t nrows_valid, int64_t nt) {
+  vfrb_dd_args a{};
+  a.fb = s->d_cm;
+  a.storage = pl->P.storage;
+  a.chan_scale = pl->P.storage == VFRB_F32 ? nullptr : s->d_w;
+  a.chan_stride = s->cm_stride;
+  a.row0 = row0;
+  a.row_mask = s->cm_mask;
+  a.nrows_valid = nrows_valid;
+  a.nt_out = nt;
+  a.out = s->d_out;
+  a.out_stride = s->out_stride;
+  a.sigma_out = want(pl, VFRB_OUT_SIGMA) ? s->d_sig : nullptr;
+  a.workspace = s->d_ws;
+  a.workspace_bytes = s->ws_bytes;
+  const bool stats = want(pl, VFRB_OUT_DMSTATS) || want(pl, VFRB_OUT_CANDS);
+  a.ave = stats ? s->d_ave : nullptr;
+  a.sigma = stats ? s->d_sgm : nullptr;
+  a.peak = stats ? s->d_peak : nullptr;
+  a.frb = stats ? s->d_frb : nullptr;
+  a.argmax = stats ? s->d_arg : nullptr;
+  a.d_err = s->d_err;
+  return launch_dedisperse_plan(pl->dd, a, s->cs);
+}
+
+// Copy this result's outputs to the host and queue it.
+int emit(vfrb_plan* pl, StreamSt* s, int64_t seq, int64_t row0, int64_t nt, bool with_fb) {
+  ResultSlot* r = nullptr;
+  ST(alloc_slot(pl, s, &r));
+  const int64_t nch = pl->L.nchanout;
+  if (pl->want_dd && nt > 0) {
+    if (want(pl, VFRB_OUT_DEDISP))
+      CK(cudaMemcpy2DAsync(r->dd, nt * 4, s->d_out, s->out_stride * 4, nt * 4, pl->ndm, cudaMemcpyDeviceToHost,
+                           s->cs));
+    if (want(pl, VFRB_OUT_SIGMA))
+      CK(cudaMemcpy2DAsync(r->dds, nt * 4, s->d_sig, s->out_stride * 4, nt * 4, pl->ndm, cudaMemcpyDeviceToHost,
+                           s->cs));
+    if (want(pl, VFRB_OUT_DMSTATS) || want(pl, VFRB_OUT_CANDS)) {
+      CK(cudaMemcpyAsync(r->ave, s->d_ave, pl->ndm * 4, cudaMemcpyDeviceToHost, s->cs));
+      CK(cudaMemcpyAsync(r->sig, s->d_sgm, pl->ndm * 4, cudaMemcpyDeviceToHost, s->cs));
+      CK(cudaMemcpyAsync(r->peak, s->d_peak, pl->ndm * 4, cudaMemcpyDeviceToHost, s->cs));
+      CK(cudaMemcpyAsync(r->frb, s->d_frb, pl->ndm * 4, cudaMemcpyDeviceToHost, s->cs));
+      CK(cudaMemcpyAsync(r->arg, s->d_arg, pl->ndm * 4, cudaMemcpyDeviceToHost, s->cs));
+    }
+  }
+  if (with_fb && r->fb) CK(cudaMemcpyAsync(r->fb, s->d_fbt, (size_t)pl->L.maxnt * nch * 4, cudaMemcpyDeviceToHost, s->cs));
+  const bool cst = pl->P.mode == VFRB_MODE_BLOCK && want(pl, VFRB_OUT_CHANSTATS);
+  if (cst) {
+    const size_t b = (size_t)pl->nstatblks * nch * 4;
+    CK(cudaMemcpyAsync(r->cave, s->d_cave, b, cudaMemcpyDeviceToHost, s->cs));
+    CK(cudaMemcpyAsync(r->csig, s->d_csig, b, cudaMemcpyDeviceToHost, s->cs));
+    CK(cudaMemcpyAsync(r->cout, s->d_cout, b, cudaMemcpyDeviceToHost, s->cs));
+  }
+  CK(cudaMemcpyAsync(r->err, s->d_err, 4, cudaMemcpyDeviceToHost, s->cs));
+  CK(cudaMemsetAsync(s->d_err, 0, 4, s->cs));
+  r->t_done = 0.0;
+  CK(cudaLaunchHostFunc(s->cs, mark_done, r));
+  CK(cudaEventRecord(r->ev, s->cs));
+  vfrb_result& o = r->r;
+  o = vfrb_result{};
+  o.stream = s->id;
+  o.seq = seq;
+  o.row0 = row0;
+  o.tstart_mjd = s->tstart_mjd;
+  o.ndm = pl->want_dd ? pl->ndm : 0;
+  o.nt = pl->want_dd ? nt : 0;
+  const bool stats = pl->want_dd && (want(pl, VFRB_OUT_DMSTATS) || want(pl, VFRB_OUT_CANDS));
+  o.dd = (pl->want_dd && want(pl, VFRB_OUT_DEDISP)) ? r->dd : nullptr;
+  o.dd_sigma = (pl->want_dd && want(pl, VFRB_OUT_SIGMA)) ? r->dds : nullptr;
+  o.ave = stats ? r->ave : nullptr;
+  o.sigma = stats ? r->sig : nullptr;
+  o.peak = stats ? r->peak : nullptr;
+  o.frb = stats ? r->frb : nullptr;
+  o.argmax = stats ? r->arg : nullptr;
+  o.nchan = (int32_t)nch;
+  o.fb_rows = (with_fb && r->fb) ? pl->L.maxnt : 0;
+  o.fb = (with_fb && r->fb) ? r->fb : nullptr;
+  o.nstatblks = cst ? pl->nstatblks : 0;
+  o.chan_ave = cst ? r->cave : nullptr;
+  o.chan_sig = cst ? r->csig : nullptr;
+  o.chan_outlier = cst ? r->cout : nullptr;
+  r->t_data = s->t_push;
+  r->state = 1;
+  pl->queue.push_back(r);
+  return VFRB_OK;
+}
+
+int block_complete(vfrb_plan* pl, StreamSt* s) {
+  const vfrb_layout& L = pl->L;
+  const int64_t nch = L.nchanout;
+  if (pl->want_dd && pl->max_delay > 0)
+    CK(cudaMemcpyAsync(s->d_left, s->d_fb_tm + (int64_t)(L.maxnt - pl->max_delay) * nch,
+                       (size_t)pl->max_delay * nch * 4, cudaMemcpyDeviceToDevice, s->cs));
+  const bool with_fb = want(pl, VFRB_OUT_FB) && (pl->P.fb_block < 0 || pl->P.fb_block == s->blocks);
+  ST(run_bandpass(pl, s, s->d_fb_tm, 0, 0xffffffffu, L.maxnt, 0, with_fb ? s->d_fbt : nullptr));
+  if (want(pl, VFRB_OUT_CHANSTATS)) {
+    vfrb_cs_args c{};
+    c.fb = (const float*)s->d_cm;
+    c.chan_stride = s->cm_stride;
+    c.row_mask = 0xffffffffu;
+    c.nchan = (int32_t)nch;
+    c.nrows = L.maxnt;
+    c.ncolstatblk = pl->ncolstatblk;
+    c.nstatblks = pl->nstatblks;
+    c.ave = s->d_cave;
+    c.sig = s->d_csig;
+    c.outlier = s->d_cout;
+    ST(launch_chan_stats(c, s->cs));
+  }
+  if (pl->want_dd) ST(run_dedisp(pl, s, 0, L.maxnt, pl->nt_block));
+  ST(emit(pl, s, s->blocks, s->blocks, pl->want_dd ? pl->nt_block : 0, with_fb));
+  if (pl->want_dd && pl->max_delay > 0) {
+    CK(cudaMemcpyAsync(s->d_fb_tm, s->d_left, (size_t)pl->max_delay * nch * 4, cudaMemcpyDeviceToDevice, s->cs));
+    s->loopcnt = pl->max_delay / L.nbundle;
+  } else {
+    s->loopcnt = 0;
+  }
+  ++s->blocks;
+  return VFRB_OK;
+}
+
+int stream_chunk(vfrb_plan* pl, StreamSt* s, int64_t nt) {
+  ST(run_dedisp(pl, s, s->rows_out, s->rows_bp - s->rows_out, nt));
+  ST(emit(pl, s, s->chunks, s->rows_out, nt, false));
+  s->rows_out += nt;
+  ++s->chunks;
+  return VFRB_OK;
+}
+
+// Turn every complete bundle / row / window into work.
+int process(vfrb_plan* pl, StreamSt* s, bool final_flush) {
+  const vfrb_layout& L = pl->L;
+  const int64_t S = (int64_t)L.nave * L.twonchan;
+  if (pl->P.mode == VFRB_MODE_BLOCK) {
+    const int64_t per_block = L.maxnt / L.nbundle;
+    for (;;) {
+      // bundle b is complete once the pair read after its last byte exists (PIPE:1143-1158)
+      int64_t nb = 0;
+      const int64_t have = npairs(s);
+      while (true) {
+        const int64_t b = s->bundles_done + nb;
+        const int64_t need = ((b + 1) * (int64_t)L.nloop) / kDataLen;
+        if (need >= have) break;
+        if (s->loopcnt + nb + 1 > per_block) break;
+        if ((nb + 1) * L.nbundle > pl->launch_rows) break;
+        ++nb;
+      }
+      if (nb == 0) break;
+      ST(launch_rows(pl, s, s->bundles_done * L.nbundle, nb * L.nbundle, s->d_fb_tm, (int64_t)s->loopcnt * L.nbundle,
+                     0xffffffffu));
+      s->bundles_done += nb;
+      s->loopcnt += (int)nb;
+      consume_entries(s, (s->bundles_done * (int64_t)L.nloop) / kDataLen);
+      if (s->loopcnt == per_block) ST(block_complete(pl, s));
+    }
+    return VFRB_OK;
+  }
+  for (;;) {
+    const int64_t avail = npairs(s) * kDataLen / S;
+    int64_t n = std::min(avail - s->rows_chan, pl->launch_rows);
+    n = std::min(n, s->R1 - 256 - (s->rows_chan - s->rows_bp));
+    if (n <= 0) break;
+    ST(launch_rows(pl, s, s->rows_chan, n, s->d_raw, s->rows_chan, (unsigned)(s->R1 - 1)));
+    s->rows_chan += n;
+    consume_entries(s, (s->rows_chan * S) / kDataLen);
+    const int64_t w1 = (s->rows_chan / 128) * 128;
+    if (w1 > s->rows_bp) {
+      ST(run_bandpass(pl, s, s->d_raw, s->rows_bp, (unsigned)(s->R1 - 1), w1 - s->rows_bp, s->rows_bp, nullptr));
+      s->rows_bp = w1;
+    }
+    if (pl->want_dd)
+      while (s->rows_bp - pl->max_delay - s->rows_out >= pl->chunk_rows) ST(stream_chunk(pl, s, pl->chunk_rows));
+  }
+  if (final_flush && pl->want_dd) {
+    const int64_t rem = s->rows_bp - pl->max_delay - s->rows_out;
+    if (rem > 0) ST(stream_chunk(pl, s, rem));
+  }
+  return VFRB_OK;
+}
+
+int run_reader(vfrb_plan* pl, StreamSt* s) {
+  const auto r = s->reader->run(s->e0, s->e1);
+  if (!s->started && s->reader->initialised()) {
+    s->started = true;
+    vfrb_hdr h = s->reader->start_header();
+    s->tstart_mjd = vfrb_header_dmjd(&h, kFramesPerSec);
+  }
+  for (auto& l : s->reader->log()) {
+    s->logtext += l;
+    s->logtext += '\n';
+  }
+  s->reader->log().clear();
+  if (r == PairReader::STEP_ERROR) s->reader_error = VFRB_ERR;
+  (void)pl;
+  return VFRB_OK;
+}
+
+// Oldest frame index still referenced by unconsumed entries or queued frames.
+int64_t oldest_ref(const StreamSt* s) {
+  int64_t o = s->frames_in - (int64_t)s->reader->queued();
+  for (size_t k = s->ehead; k < s->e0.size(); ++k) {
+    if (s->e0[k] >= 0) o = std::min(o, s->e0[k]);
+    if (s->e1[k] >= 0) o = std::min(o, s->e1[k]);
+    if (s->e0[k] >= 0 && s->e1[k] >= 0) break;  // entries are in read order
+  }
+  return o;
+}
+
+// Copy `nf` whole frames to the ring, queue their headers, advance.
+int feed_frames(vfrb_plan* pl, StreamSt* s, const uint8_t* host, int64_t nf, bool pinned) {
+  const int64_t batch_max = std::max<int64_t>(1, std::min<int64_t>(s->ring_frames / 4, (int64_t)s->stage_frames));
+  for (int64_t done = 0; done < nf;) {
+    const int64_t nb = std::min(batch_max, nf - done);
+    const uint8_t* src = host + done * kFrameLen;
+    // frames about to be overwritten must have been consumed by launched work
+    if (oldest_ref(s) < s->frames_in + nb - s->ring_frames) {
+      ST(process(pl, s, false));
+      if (oldest_ref(s) < s->frames_in + nb - s->ring_frames) return VFRB_ERR_NOMEM;  // ring too small
+    }
+    CK(cudaStreamWaitEvent(s->xs, s->ev_consumed, 0));
+    const uint8_t* from = src;
+    if (!pinned) {
+      const int k = s->stage_i;
+      s->stage_i = (s->stage_i + 1) % kStageBufs;
+      CK(cudaEventSynchronize(s->stage_ev[k]));
+      std::memcpy(s->h_stage[k], src, (size_t)nb * kFrameLen);
+      from = s->h_stage[k];
+      // the staging event is recorded after the copies below
+      const int64_t slot0 = s->frames_in % s->ring_frames;
+      const int64_t n1 = std::min(nb, s->ring_frames - slot0);
+      CK(cudaMemcpyAsync(s->d_frames + slot0 * kFrameLen, from, (size_t)n1 * kFrameLen, cudaMemcpyHostToDevice, s->xs));
+      if (nb > n1)
+        CK(cudaMemcpyAsync(s->d_frames, from + n1 * kFrameLen, (size_t)(nb - n1) * kFrameLen, cudaMemcpyHostToDevice,
+                           s->xs));
+      CK(cudaEventRecord(s->stage_ev[k], s->xs));
+    } else {
+      const int64_t slot0 = s->frames_in % s->ring_frames;
+      const int64_t n1 = std::min(nb, s->ring_frames - slot0);
+      CK(cudaMemcpyAsync(s->d_frames + slot0 * kFrameLen, from, (size_t)n1 * kFrameLen, cudaMemcpyHostToDevice, s->xs));
+      if (nb > n1)
+        CK(cudaMemcpyAsync(s->d_frames, from + n1 * kFrameLen, (size_t)(nb - n1) * kFrameLen, cudaMemcpyHostToDevice,
+                           s->xs));
+    }
+    CK(cudaEventRecord(s->ev_copied, s->xs));
+    CK(cudaStreamWaitEvent(s->cs, s->ev_copied, 0));
+    for (int64_t i = 0; i < nb; ++i) {
+      QFrame q;
+      vfrb_decode_header(src + i * kFrameLen, &q.h);
+      q.payload = s->frames_in + i;
+      s->reader->push(q);
+    }
+    s->frames_in += nb;
+    ST(run_reader(pl, s));
+    ST(process(pl, s, false));
+    done += nb;
+  }
+  if (pinned) CK(cudaEventSynchronize(s->ev_copied));  // the caller may reuse its buffer on return
+  return VFRB_OK;
+}
+
+int free_plan(vfrb_plan* pl) {
+  if (!pl) return VFRB_OK;
+  for (auto s : pl->streams) cudaStreamSynchronize(s);
+  for (auto s : pl->streams) cudaStreamDestroy(s);
+  for (auto e : pl->events) cudaEventDestroy(e);
+  for (auto p : pl->dev_allocs) cudaFree(p);
+  for (auto p : pl->host_allocs) cudaFreeHost(p);
+  if (pl->dd) ddplan_destroy(pl->dd);
+  delete pl;
+  return VFRB_OK;
+}
+
+int create_stream(vfrb_plan* pl, int id, int64_t ring_frames, int64_t R1, int64_t R2) {
+  auto s = std::make_unique<StreamSt>();
+  const vfrb_params& P = pl->P;
+  const vfrb_layout& L = pl->L;
+  const int64_t nch = L.nchanout;
+  s->id = id;
+  s->reader = std::make_unique<PairReader>(P.reader == VFRB_READER_TS ? PairReader::TS : PairReader::PIPE,
+                                           P.dada_skip != 0);
+  CK(cudaStreamCreateWithFlags(&s->cs, cudaStreamNonBlocking));
+  pl->streams.push_back(s->cs);
+  CK(cudaStreamCreateWithFlags(&s->xs, cudaStreamNonBlocking));
+  pl->streams.push_back(s->xs);
+  ST(mkevent(pl, &s->ev_copied));
+  ST(mkevent(pl, &s->ev_consumed));
+  CK(cudaEventRecord(s->ev_consumed, s->cs));
+  s->ring_frames = ring_frames;
+  ST(dmalloc(pl, &s->d_frames, (size_t)ring_frames * kFrameLen + (size_t)kStash * kDataLen));
+  s->stage_frames = (size_t)std::min<int64_t>(ring_frames / 4, 8192);
+  for (int k = 0; k < kStageBufs; ++k) {
+    ST(hmalloc(pl, &s->h_stage[k], s->stage_frames * kFrameLen));
+    ST(mkevent(pl, &s->stage_ev[k]));
+    CK(cudaEventRecord(s->stage_ev[k], s->xs));
+  }
+  s->slots_cap = (pl->launch_rows * L.nave * (int64_t)L.twonchan) / kDataLen + 4;
+  for (auto& b : s->sb) {
+    ST(hmalloc(pl, &b.h, sizeof(int64_t) * 2 * s->slots_cap));
+    ST(dmalloc(pl, &b.d, sizeof(int64_t) * 2 * s->slots_cap));
+    ST(mkevent(pl, &b.ev));
+    CK(cudaEventRecord(b.ev, s->cs));
+  }
+  ST(dmalloc(pl, &s->d_err, 4));
+  CK(cudaMemsetAsync(s->d_err, 0, 4, s->cs));
+  ST(dmalloc(pl, &s->d_w, nch * 4));
+  ST(dmalloc(pl, &s->d_inv, nch * 4));
+  ST(dmalloc(pl, &s->d_var, nch * 4));
+  ST(dmalloc(pl, &s->d_scr, nch * 128 * 4));
+  const size_t sb = storage_bytes(P.storage);
+  int64_t nt = 0;
+  if (P.mode == VFRB_MODE_BLOCK) {
+    ST(dmalloc(pl, &s->d_fb_tm, (size_t)L.maxnt * nch * 4));
+    CK(cudaMemsetAsync(s->d_fb_tm, 0, (size_t)L.maxnt * nch * 4, s->cs));
+    if (pl->want_dd && pl->max_delay > 0) ST(dmalloc(pl, &s->d_left, (size_t)pl->max_delay * nch * 4));
+    s->cm_stride = ((int64_t)L.maxnt + 15) / 16 * 16;
+    s->cm_mask = 0xffffffffu;
+    ST(dmalloc(pl, &s->d_cm, (size_t)nch * s->cm_stride * sb));
+    if (want(pl, VFRB_OUT_FB)) ST(dmalloc(pl, &s->d_fbt, (size_t)L.maxnt * nch * 4));
+    if (want(pl, VFRB_OUT_CHANSTATS)) {
+      ST(dmalloc(pl, &s->d_cave, (size_t)pl->nstatblks * nch * 4));
+      ST(dmalloc(pl, &s->d_csig, (size_t)pl->nstatblks * nch * 4));
+      ST(dmalloc(pl, &s->d_cout, (size_t)pl->nstatblks * nch * 4));
+    }
+    nt = pl->nt_block;
+  } else {
+    s->R1 = R1;
+    ST(dmalloc(pl, &s->d_raw, (size_t)R1 * nch * 4));
+    s->cm_stride = R2;
+    s->cm_mask = (unsigned)(R2 - 1);
+    ST(dmalloc(pl, &s->d_cm, (size_t)nch * R2 * sb));
+    CK(cudaMemsetAsync(s->d_cm, 0, (size_t)nch * R2 * sb, s->cs));
+    nt = pl->chunk_rows;
+  }
+  if (pl->want_dd) {
+    s->out_stride = nt;
+    ST(dmalloc(pl, &s->d_out, (size_t)pl->ndm * nt * 4));
+    if (want(pl, VFRB_OUT_SIGMA)) ST(dmalloc(pl, &s->d_sig, (size_t)pl->ndm * nt * 4));
+    ST(dmalloc(pl, &s->d_ave, pl->ndm * 4));
+    ST(dmalloc(pl, &s->d_sgm, pl->ndm * 4));
+    ST(dmalloc(pl, &s->d_peak, pl->ndm * 4));
+    ST(dmalloc(pl, &s->d_frb, pl->ndm * 4));
+    ST(dmalloc(pl, &s->d_arg, pl->ndm * 4));
+    s->ws_bytes = dedisperse_workspace_bytes_plan(pl->dd, nt);
+    ST(dmalloc(pl, &s->d_ws, s->ws_bytes));
+  }
+  StreamSt* sp = s.get();
+  // a gap-revealing frame is copied aside: it is used again NSKIP pairs later
+  s->reader->on_gap = [pl, sp](int64_t v) -> int64_t {
+    if (v < 0) return v;
+    const int k = sp->stash_next;
+    sp->stash_next = (sp->stash_next + 1) % kStash;
+    const uint8_t* from = sp->d_frames + (v % sp->ring_frames) * kFrameLen + kHdrLen;
+    uint8_t* to = sp->d_frames + sp->ring_frames * kFrameLen + (int64_t)k * kDataLen;
+    if (cudaMemcpyAsync(to, from, kDataLen, cudaMemcpyDeviceToDevice, sp->cs) != cudaSuccess) {
+      cudaGetLastError();
+      sp->reader_error = VFRB_ERR_CUDA;
+    }
+    (void)pl;
+    return -2 - k;
+  };
+  pl->st.push_back(std::move(s));
+  return VFRB_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+void vfrb_params_default(vfrb_params* p) {
+  if (!p) return;
+  std::memset(p, 0, sizeof(*p));
+  p->twonchan = 12500;
+  p->nave = 4;
+  p->nbundle = 32;
+  p->muoslowfreq = 360.0;
+  p->maxtime = 70.f;
+  p->timestats = 1.f;
+  p->mode = VFRB_MODE_BLOCK;
+  p->reader = VFRB_READER_PIPE;
+  p->storage = VFRB_F32;
+  p->q_scale = 16.f;
+  p->outputs = VFRB_OUT_DEDISP | VFRB_OUT_DMSTATS;
+  p->fb_block = -1;
+  p->nstreams = 1;
+  p->chunk_seconds = 1.f;
+  p->ring_seconds = 1.f;
+  p->cand_snr = 6.f;
+}
+
+int vfrb_plan_create(vfrb_plan** out, const vfrb_params* prm) {
+  if (!out || !prm) return VFRB_ERR_ARG;
+  *out = nullptr;
+  vfrb_plan* pl = new vfrb_plan();
+  pl->P = *prm;
+  vfrb_params& P = pl->P;
+  auto fail = [&](int st) {
+    free_plan(pl);
+    return st;
+  };
+  if (P.nstreams < 1 || P.nstreams > 4096 || (P.mode != VFRB_MODE_BLOCK && P.mode != VFRB_MODE_STREAM) ||
+      P.storage < VFRB_F32 || P.storage > VFRB_I8 || P.ring_seconds <= 0.f || P.q_scale <= 0.f)
+    return fail(VFRB_ERR_ARG);
+  if (cudaSetDevice(P.device) != cudaSuccess) return fail(VFRB_ERR_CUDA);
+  int st = vfrb_layout_init(&pl->L, P.twonchan, P.nave, P.nbundle, P.muoslowfreq, P.nchanout_fixed, P.maxtime);
+  if (st) return fail(st);
+  const vfrb_layout& L = pl->L;
+  if (L.twonchan != kFftN) return fail(VFRB_ERR_UNSUPPORTED);
+  pl->want_dd = (P.outputs & (VFRB_OUT_DEDISP | VFRB_OUT_DMSTATS | VFRB_OUT_SIGMA | VFRB_OUT_CANDS)) != 0;
+  if (pl->want_dd) {
+    if (P.ndm < 1 || !P.dms) return fail(VFRB_ERR_ARG);
+    pl->ndm = P.ndm;
+    pl->dms.assign(P.dms, P.dms + P.ndm);
+    pl->off.resize((size_t)P.ndm * L.nchanout);
+    int32_t mdf = 0;
+    st = vfrb_delay_table(&L, pl->dms.data(), P.ndm, pl->off.data(), &mdf);
+    if (st) return fail(st);
+    st = ddplan_create(&pl->dd, pl->off.data(), P.ndm, L.nchanout);
+    if (st) return fail(st);
+    const int tmax = ddplan_max_delay(pl->dd);
+    if (P.mode == VFRB_MODE_BLOCK) {
+      // the reference's carry uses the TS:464 formula with the LAST list entry
+      if (mdf < tmax) return fail(VFRB_ERR_ARG);  // DM list must end with its largest trial
+      pl->max_delay = mdf;
+    } else {
+      pl->max_delay = tmax;
+    }
+  }
+  if (P.mode == VFRB_MODE_BLOCK) {
+    if (L.maxnt % L.nbundle != 0) return fail(VFRB_ERR_UNSUPPORTED);  // rows past the last bundle are never written
+    if (pl->want_dd && L.maxnt <= pl->max_delay) return fail(VFRB_ERR_ARG);
+    pl->nt_block = pl->want_dd ? L.maxnt - pl->max_delay : 0;
+    if (P.outputs & VFRB_OUT_CHANSTATS) {
+      pl->nstatblks = (int)(P.maxtime / P.timestats);          // STATS:210
+      pl->ncolstatblk = (int)((double)P.timestats / L.tchan);  // STATS:211
+      if (pl->nstatblks < 1 || pl->ncolstatblk < 2 || (int64_t)pl->ncolstatblk * (pl->nstatblks - 1) >= L.maxnt)
+        return fail(VFRB_ERR_ARG);
+      if (P.storage != VFRB_F32) return fail(VFRB_ERR_UNSUPPORTED);
+    }
+  } else {
+    pl->chunk_rows = std::max<int64_t>(32, (int64_t)llround(P.chunk_seconds / L.tchan));
+  }
+  const int64_t S = (int64_t)L.nave * L.twonchan;
+  int64_t ring_frames = std::max<int64_t>(4 * (2 * kFramesPerCal + 16), (int64_t)(P.ring_seconds * kFramesPerSec * 2));
+  ring_frames += ring_frames & 1;
+  pl->launch_rows = std::max<int64_t>(L.nbundle, ((ring_frames / 8) * kDataLen) / S / L.nbundle * L.nbundle);
+  const int64_t R1 = (int64_t)pow2_at_least((unsigned long long)(pl->launch_rows + 512));
+  const int64_t R2 = (int64_t)pow2_at_least(
+      (unsigned long long)(pl->max_delay + pl->chunk_rows + pl->launch_rows + 512));
+  // admission by device memory
+  const int64_t need = stream_bytes(pl, ring_frames, R1, R2) * P.nstreams;
+  size_t fr = 0, tot = 0;
+  if (cudaMemGetInfo(&fr, &tot) != cudaSuccess) return fail(VFRB_ERR_CUDA);
+  const int64_t budget = P.device_bytes > 0 ? P.device_bytes : (int64_t)(0.9 * (double)fr);
+  if (need > budget) return fail(VFRB_ERR_NOMEM);
+  for (int i = 0; i < P.nstreams; ++i) {
+    st = create_stream(pl, i, ring_frames, R1, R2);
+    if (st) return fail(st);
+  }
+  for (auto& s : pl->st)
+    if (cudaStreamSynchronize(s->cs) != cudaSuccess || cudaStreamSynchronize(s->xs) != cudaSuccess)
+      return fail(VFRB_ERR_CUDA);
+  *out = pl;
+  return VFRB_OK;
+}
+
+int vfrb_plan_destroy(vfrb_plan* pl) { return free_plan(pl); }
+
+int vfrb_plan_layout(const vfrb_plan* pl, vfrb_layout* L, int32_t* max_delay) {
+  if (!pl) return VFRB_ERR_ARG;
+  if (L) *L = pl->L;
+  if (max_delay) *max_delay = pl->max_delay;
+  return VFRB_OK;
+}
+
+int64_t vfrb_plan_device_bytes(const vfrb_plan* pl) { return pl ? pl->dev_bytes : -1; }
+
+int vfrb_push_frames(vfrb_plan* pl, int stream, const uint8_t* bytes, size_t nbytes) {
+  if (!pl || stream < 0 || stream >= (int)pl->st.size()) return VFRB_ERR_ARG;
+  StreamSt* s = pl->st[stream].get();
+  if (s->ended) return VFRB_ERR_ARG;
+  if (s->reader_error) return s->reader_error;
+  if (cudaSetDevice(pl->P.device) != cudaSuccess) return VFRB_ERR_CUDA;
+  s->t_push = now_ms();
+  if (nbytes == 0 || !bytes) {  // end of data: the incomplete frame is dropped, as fread would fail on it
+    s->part.clear();
+    s->reader->end_of_data();
+    ST(run_reader(pl, s));
+    ST(process(pl, s, true));
+    s->ended = true;
+    return s->reader_error;
+  }
+  const bool pinned = is_pinned(bytes);
+  size_t pos = 0;
+  if (!s->part.empty()) {
+    const size_t take = std::min(nbytes, (size_t)kFrameLen - s->part.size());
+    s->part.insert(s->part.end(), bytes, bytes + take);
+    pos = take;
+    if (s->part.size() == (size_t)kFrameLen) {
+      ST(feed_frames(pl, s, s->part.data(), 1, false));
+      s->part.clear();
+    }
+  }
+  const int64_t whole = (int64_t)((nbytes - pos) / kFrameLen);
+  if (whole > 0) ST(feed_frames(pl, s, bytes + pos, whole, pinned));
+  pos += (size_t)whole * kFrameLen;
+  if (pos < nbytes) s->part.assign(bytes + pos, bytes + nbytes);
+  return s->reader_error;
+}
+
+int vfrb_poll(vfrb_plan* pl, vfrb_result* out, int wait) {
+  if (!pl || !out) return VFRB_ERR_ARG;
+  if (pl->held) {
+    pl->held->state = 0;
+    pl->held = nullptr;
+  }
+  if (pl->queue.empty()) {
+    for (auto& s : pl->st)
+      if (!s->ended) return VFRB_PENDING;
+    return VFRB_EOD;
+  }
+  auto it = pl->queue.begin();
+  for (; it != pl->queue.end(); ++it) {
+    const cudaError_t q = cudaEventQuery((*it)->ev);
+    if (q == cudaSuccess) break;
+    if (q != cudaErrorNotReady) return VFRB_ERR_CUDA;
+  }
+  if (it == pl->queue.end()) {
+    if (!wait) return VFRB_PENDING;
+    it = pl->queue.begin();
+    if (cudaEventSynchronize((*it)->ev) != cudaSuccess) return VFRB_ERR_CUDA;
+  }
+  ResultSlot* r = *it;
+  pl->queue.erase(it);
+  r->state = 2;
+  pl->held = r;
+  vfrb_result& o = r->r;
+  o.latency_ms = r->t_done - r->t_data;
+  o.device_errors = *r->err;
+  r->cands.clear();
+  if (o.peak && o.argmax && (pl->P.outputs & VFRB_OUT_CANDS)) {
+    // candidates: per DM the chunk's peak SNR (calcstats semantics) above the
+    // threshold, kept where it is a local maximum over neighbouring trials
+    for (int d = 0; d < o.ndm; ++d) {
+      const float p = o.peak[d];
+      if (!(p >= pl->P.cand_snr)) continue;
+      if (d > 0 && o.peak[d - 1] > p) continue;
+      if (d + 1 < o.ndm && o.peak[d + 1] >= p) continue;
+      vfrb_cand c;
+      c.dm_index = d;
+      c.width = 1;
+      c.t = o.row0 + o.argmax[d];
+      c.snr = p;
+      c.dm = pl->dms[d];
+      r->cands.push_back(c);
+    }
+  }
+  o.ncand = (int32_t)r->cands.size();
+  o.cands = r->cands.empty() ? nullptr : r->cands.data();
+  *out = o;
+  return VFRB_OK;
+}
+
+const char* vfrb_stream_log(vfrb_plan* pl, int stream) {
+  if (!pl || stream < 0 || stream >= (int)pl->st.size()) return "";
+  pl->logtmp = pl->st[stream]->logtext;
+  return pl->logtmp.c_str();
+}
+
+}  // extern "C"

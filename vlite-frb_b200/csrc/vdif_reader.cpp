@@ -1,0 +1,187 @@
+// Pol-pair reader state machine (see vdif_reader.h).
+#include "vdif_reader.h"
+#include "vfrb_common.cuh"
+
+#include <algorithm>
+#include <cstdio>
+
+namespace vfrb {
+
+bool PairReader::read_raw(int p) {
+  if (q_.empty()) return false;
+  hdr_[p] = q_.front().h;
+  cur_[p] = q_.front().payload;
+  q_.pop_front();
+  return true;
+}
+
+// checkframeskip0/1: PIPE:888-930 (frame number mod 25600) and TS:895-937
+// (seconds-aware; a negative gap leaves the pol on fill frames for good, as
+// the reference's NSKIP countdown never reaches zero).
+void PairReader::checkframeskip(int p) {
+  const int fnum = (int)hdr_[p].frame;
+  if (mode_ == TS) {
+    const long long fsec = hdr_[p].seconds;
+    if (fnum != expected_[p] || fsec != expsec_[p]) {
+      nskip_[p] = (long long)fnum - expected_[p] + (fsec - expsec_[p]) * kFramesPerSec;
+      tmp_[p] = on_gap ? on_gap(cur_[p]) : cur_[p];
+      cur_[p] = kFill;
+      char b[160];
+      snprintf(b, sizeof b, "FRAME SKIP %d: expected %lld %d, read %lld %d (NSKIP=%lld)", p, expsec_[p], expected_[p],
+               fsec, fnum, nskip_[p]);
+      log_.emplace_back(b);
+    }
+    expected_[p] = (fnum + 1) % kFramesPerSec;
+    expsec_[p] = fsec + (expected_[p] == 0 ? 1 : 0);
+  } else {
+    if (fnum != expected_[p]) {
+      long long n = (long long)fnum - expected_[p];
+      if (n < 0) n += kFramesPerSec;
+      nskip_[p] = n;
+      tmp_[p] = on_gap ? on_gap(cur_[p]) : cur_[p];
+      cur_[p] = kFill;
+      char b[160];
+      snprintf(b, sizeof b, "FRAME SKIP %d: expected %d, read %d (NSKIP=%lld)", p, expected_[p], fnum, n);
+      log_.emplace_back(b);
+    }
+    expected_[p] = (fnum + 1) % kFramesPerSec;
+  }
+}
+
+// readoneframePOL0/1 (PIPE:934-1025)
+bool PairReader::readone(int p) {
+  if (nskip_[p]) {
+    nskip_[p]--;
+    if (nskip_[p] == 0) cur_[p] = tmp_[p];
+    return true;
+  }
+  if (!read_raw(p)) return false;
+  checkframeskip(p);
+  return true;
+}
+
+// initframe01 (PIPE:1058-1131; TS:1070-1145).  0 ok, 1 abort/retry, 2 error.
+int PairReader::initframe01() {
+  if (!read_raw(0)) return 1;
+  if (hdr_[0].threadid != 0) {
+    log_.emplace_back("VDIF Threads misaligned, skipping forward 1 frame");
+    if (!read_raw(0)) return 1;
+  }
+  if (hdr_[0].threadid != 0) return 1;
+  if (!read_raw(1)) return 1;
+  if (hdr_[1].threadid != 1) return 1;
+  const bool ts = mode_ == TS;
+  int fnum0 = (int)hdr_[0].frame;
+  int fnum1 = (int)hdr_[1].frame;
+  if (fnum0 != fnum1 || (ts && hdr_[0].seconds != hdr_[1].seconds)) return ts ? 2 : 1;
+  long long ncal = 0;
+  while (fnum0 % kFramesPerCal != 0) {  // fmod((float)fnum0, 2560.f) < 1e-4, exact below 2^24
+    if (!read_raw(0)) return 1;
+    if (!read_raw(1)) return 1;
+    fnum0 = (int)hdr_[0].frame;
+    ++ncal;
+  }
+  fnum1 = (int)hdr_[1].frame;
+  if (fnum0 != fnum1 || (ts && hdr_[0].seconds != hdr_[1].seconds)) return ts ? 2 : 1;
+  char b[96];
+  snprintf(b, sizeof b, "Skipped %lld frames to begin at noise cal cycle", ncal);
+  log_.emplace_back(b);
+  for (int p = 0; p < 2; ++p) {
+    expected_[p] = ((int)hdr_[p].frame + 1) % kFramesPerSec;
+    expsec_[p] = (long long)hdr_[p].seconds + (expected_[p] == 0 ? 1 : 0);
+  }
+  return 0;
+}
+
+PairReader::Status PairReader::run(std::vector<int64_t>& e0, std::vector<int64_t>& e1) {
+  if (phase_ == DONE) return failed_ ? STEP_EOD : STEP_ERROR;
+  if (phase_ == INIT && dada_skip_ && skipped_ == 0) phase_ = DADA_SKIP;
+  if (phase_ == DADA_SKIP) {  // initDADA: discard NFRAMEDADAINIT frame pairs (TS:767-826)
+    while (skipped_ < kDadaInitFrames) {
+      if (q_.size() < 2) {
+        if (!eod_) return STEP_NEED;
+        phase_ = DONE;
+        failed_ = true;
+        return STEP_EOD;
+      }
+      q_.pop_front();
+      q_.pop_front();
+      ++skipped_;
+    }
+    phase_ = INIT;
+    dada_skip_ = false;
+  }
+  if (phase_ == INIT) {
+    // initframe01 consumes at most 2 + 1 + 2*2559 + 1 frames: wait until they are queued.
+    constexpr size_t kInitNeed = 2 * kFramesPerCal + 8;
+    for (;;) {
+      if (q_.size() < kInitNeed && !eod_) return STEP_NEED;
+      const int r = initframe01();
+      if (r == 0) {
+        phase_ = RUNNING;
+        start_hdr_ = hdr_[0];
+        e0.push_back(cur_[0]);
+        e1.push_back(cur_[1]);
+        break;
+      }
+      // PIPE/STATS exit with 2 on any failure (PIPE:513-516); TS retries on 1 (TS:516-523) and
+      // would spin for ever at end of data -- here the retry stops there.
+      if (mode_ != TS || r == 2) {
+        phase_ = DONE;
+        return STEP_ERROR;
+      }
+      if (q_.empty() && eod_) {
+        phase_ = DONE;
+        failed_ = true;
+        return STEP_EOD;
+      }
+    }
+  }
+  for (;;) {  // readtwoframe (PIPE:1031-1040), one pair per step
+    if (q_.size() < 2 && !eod_) return STEP_NEED;
+    if (!readone(0) || !readone(1)) {
+      phase_ = DONE;
+      failed_ = true;
+      return STEP_EOD;
+    }
+    e0.push_back(cur_[0]);
+    e1.push_back(cur_[1]);
+  }
+}
+
+}  // namespace vfrb
+
+extern "C" int vfrb_read_pairs(const uint8_t* bytes, size_t nbytes, int reader_mode, int dada_skip, size_t split,
+                               int64_t* e0, int64_t* e1, int64_t cap, int64_t* npairs, double* tstart_mjd) {
+  using namespace vfrb;
+  if ((!bytes && nbytes) || !npairs || (cap > 0 && (!e0 || !e1))) return VFRB_ERR_ARG;
+  PairReader r(reader_mode == VFRB_READER_TS ? PairReader::TS : PairReader::PIPE, dada_skip != 0);
+  std::vector<int64_t> a, b;
+  const size_t nfr = nbytes / kFrameLen;  // a trailing partial frame cannot be read
+  if (split == 0) split = nbytes ? nbytes : 1;
+  const size_t per = std::max<size_t>(1, split / kFrameLen);
+  PairReader::Status st = PairReader::STEP_NEED;
+  for (size_t k = 0; k < nfr; ++k) {
+    QFrame q;
+    vfrb_decode_header(bytes + k * kFrameLen, &q.h);
+    q.payload = (int64_t)k;
+    r.push(q);
+    if ((k + 1) % per == 0) st = r.run(a, b);
+    if (st == PairReader::STEP_ERROR) break;
+  }
+  if (st != PairReader::STEP_ERROR) {
+    r.end_of_data();
+    st = r.run(a, b);
+  }
+  const int64_t n = (int64_t)a.size();
+  *npairs = n;
+  for (int64_t i = 0; i < n && i < cap; ++i) {
+    e0[i] = a[i];
+    e1[i] = b[i];
+  }
+  if (tstart_mjd) {
+    vfrb_hdr h = r.start_header();
+    *tstart_mjd = r.initialised() || r.failed() ? vfrb_header_dmjd(&h, kFramesPerSec) : 0.0;
+  }
+  return st == PairReader::STEP_ERROR ? VFRB_ERR : VFRB_OK;
+}

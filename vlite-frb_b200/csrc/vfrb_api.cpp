@@ -11,6 +11,7 @@ int launch_dedisperse_plan(const vfrb_ddplan* pl, const vfrb_dd_args& a, cudaStr
 int ddplan_create(vfrb_ddplan** out, const int32_t* h_off, int ndm, int nchan);
 int ddplan_destroy(vfrb_ddplan* p);
 int ddplan_max_delay(const vfrb_ddplan* p);
+int ddplan_reg_group(const vfrb_ddplan* p);
 }  // namespace vfrb
 
 extern "C" {
@@ -140,6 +141,8 @@ int vfrb_ddplan_create(vfrb_ddplan** plan, const int32_t* h_offsets, int ndm, in
 int vfrb_ddplan_destroy(vfrb_ddplan* plan) { return vfrb::ddplan_destroy(plan); }
 
 int vfrb_ddplan_max_delay(const vfrb_ddplan* plan) { return plan ? vfrb::ddplan_max_delay(plan) : -1; }
+
+int vfrb_ddplan_group_size(const vfrb_ddplan* plan) { return plan ? vfrb::ddplan_reg_group(plan) : -1; }
 
 size_t vfrb_dedisperse_workspace_bytes(const vfrb_ddplan* plan, int64_t nt_out) {
   return plan ? vfrb::dedisperse_workspace_bytes_plan(plan, nt_out) : 0;
