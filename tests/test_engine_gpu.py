@@ -1,0 +1,191 @@
+"""End-to-end parity of the plan/stream engine against the oracle chain.
+
+Tolerances: dedispersed series max |gpu - oracle| <= 5e-5 * rms(oracle)
+(FP32 channeliser + FP32 sums against FP64); per-DM ave/sigma relative
+<= 1e-4, peak relative <= 1e-3, FRB flags identical; per-channel stats
+relative <= 1e-4.  Streaming results are bit-identical however the input is
+split and whether a stream runs alone or among others.
+"""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def _vdif(duration, seed=0, pulses=(), **kw):
+    from vlite_frb_b200 import synth
+    ps = [synth.Pulse(*p) for p in pulses]
+    return synth.make_vdif(synth.StreamSpec(duration=duration, seed=seed, pulses=ps, **kw)).numpy()
+
+
+@pytest.fixture(scope="module")
+def co():
+    from coracle import COracle
+    return COracle(64)
+
+
+def _oracle_rows(O, co, buf, L, mode="pipe"):
+    """FB rows of every bundle the reference would process (raw, FP64)."""
+    _, bundles, _ = O.read_bundles(buf, L, mode=mode)
+    if not bundles:
+        return np.zeros((0, L.nchanout))
+    p0 = np.concatenate([b[0] for b in bundles])
+    p1 = np.concatenate([b[1] for b in bundles])
+    return co.channelise(p0, p1, L)
+
+
+def _close(got, ref, tol, what):
+    rms = np.sqrt(np.mean(ref ** 2))
+    e = np.max(np.abs(got - ref)) / rms
+    print(f"{what}: max err / rms = {e:.2e}")
+    assert e <= tol, (what, e)
+
+
+def test_block_mode_pipe_chain(vf, O, co):
+    """PIPE semantics: MAXTIME blocks, leftover carry, block-relative BP,
+    in-tree dedisperse + calcstats (PIPE:556-708)."""
+    nave, maxtime = 2, 0.8
+    dms = np.arange(0, 10.5, 0.5, dtype=np.float32)
+    buf = _vdif(2.0, seed=11, pulses=[(0.7, 6.0, 2.0, 40.0)])
+    plan = vf.Plan(dms, nave=nave, muoslowfreq=384.0, maxtime=maxtime, mode=vf.MODE_BLOCK,
+                   outputs=vf.OUT_DEDISP | vf.OUT_DMSTATS | vf.OUT_FB, fb_block=1)
+    plan.push(0, buf)
+    plan.push(0, None)
+    res = plan.drain()
+    L = O.Layout(nave=nave, muoslowfreq=384.0, maxtime=maxtime)
+    off, md = O.delay_table(dms, L.fch1, L.chanbw, L.tchan, L.nchanout)
+    assert md == plan.max_delay
+    rows = _oracle_rows(O, co, buf, L)
+    blocks = list(O.run_blocks(rows, L, md))
+    assert len(res) == len(blocks) == 2
+    for r, (q, fb) in zip(res, blocks):
+        bp = co.bandpass(fb)
+        dd = co.dedisperse_cm(co.transpose(bp), off, L.maxnt - md)
+        _close(r["dd"], dd, 5e-5, f"block {q} dedispersed")
+        st = O.calcstats_dm(dd)
+        assert np.array_equal(r["frb"], st["frb"])
+        assert np.allclose(r["sigma"], st["sigma"], rtol=1e-4)
+        assert np.allclose(r["peak"], st["peak"], rtol=1e-3)
+        if q == 1:
+            assert r["fb"] is not None
+            _close(r["fb"], bp, 5e-5, "block 1 bandpassed FB")
+        else:
+            assert r["fb"] is None
+
+
+def test_block_mode_ts_chain(vf, O, co):
+    """TS semantics: 3840 channels, DM {0, 119.3}, dedisperseSTATS sigma."""
+    dms = np.array([0.0, 119.3], np.float32)
+    nave, maxtime = 1, 0.4
+    buf = _vdif(1.6, seed=5)
+    plan = vf.Plan(dms, nave=nave, nchanout_fixed=3840, maxtime=maxtime, mode=vf.MODE_BLOCK,
+                   reader=vf.READER_TS, outputs=vf.OUT_DEDISP | vf.OUT_SIGMA)
+    plan.push(0, buf)
+    plan.push(0, None)
+    res = plan.drain()
+    L = O.Layout(nave=nave, nchanout_fixed=3840, maxtime=maxtime)
+    off, md = O.delay_table(dms, L.fch1, L.chanbw, L.tchan, L.nchanout)
+    rows = _oracle_rows(O, co, buf, L, mode="ts")
+    blocks = list(O.run_blocks(rows, L, md))
+    assert len(res) == len(blocks) >= 2
+    for r, (q, fb) in zip(res, blocks):
+        bp = co.bandpass(fb)
+        a, s = co.dedisperse_sigma_cm(co.transpose(bp), off, L.maxnt - md)
+        _close(r["dd"], a, 5e-5, f"TS block {q} mean")
+        assert np.max(np.abs(r["dd_sigma"] - s) / s) <= 1e-4
+
+
+def test_block_mode_stats_chain(vf, O, co):
+    """STATS semantics: no overlap, per-channel stats per TIMESTATS block."""
+    nave, maxtime, tstat = 4, 0.5, 0.1
+    buf = _vdif(1.3, seed=9)
+    plan = vf.Plan(None, nave=nave, maxtime=maxtime, timestats=tstat, mode=vf.MODE_BLOCK,
+                   outputs=vf.OUT_CHANSTATS)
+    plan.push(0, buf)
+    plan.push(0, None)
+    res = plan.drain()
+    L = O.Layout(nave=nave, maxtime=maxtime)
+    rows = _oracle_rows(O, co, buf, L)
+    ncol = int(tstat / L.tchan)
+    nblk = int(np.float32(maxtime) / np.float32(tstat))
+    blocks = list(O.run_stats_blocks(rows, L))
+    assert len(res) == len(blocks) == 2
+    for r, (q, fb) in zip(res, blocks):
+        bp = co.bandpass(fb)
+        a, s, o = O.calcstats_chan(bp, ncol, nblk)
+        assert np.max(np.abs(r["chan_ave"] - a)) <= 1e-4 * np.abs(bp).max()
+        assert np.max(np.abs(r["chan_sig"] - s) / s) <= 1e-4
+        assert np.array_equal(r["chan_outlier"], o)
+
+
+def _stream_run(vf, dms, bufs, storage=0, chunk=0.25, splits=None, order=None, **kw):
+    plan = vf.Plan(dms, nave=2, muoslowfreq=384.0, mode=vf.MODE_STREAM, storage=storage, chunk_seconds=chunk,
+                   nstreams=len(bufs), outputs=vf.OUT_DEDISP | vf.OUT_DMSTATS | vf.OUT_CANDS, **kw)
+    rng = np.random.default_rng(0)
+    pos = [0] * len(bufs)
+    live = list(range(len(bufs)))
+    while live:
+        s = live[rng.integers(len(live))] if order is None else live[0]
+        n = splits(rng) if splits else len(bufs[s])
+        plan.push(s, bufs[s][pos[s]:pos[s] + n])
+        pos[s] += n
+        if pos[s] >= len(bufs[s]):
+            plan.push(s, None)
+            live.remove(s)
+    res = plan.drain()
+    per = {}
+    for r in res:
+        per.setdefault(r["stream"], []).append(r)
+    return plan, per
+
+
+def test_stream_mode_matches_oracle(vf, O, co):
+    """Streaming: absolute 128-row BP windows, every sample dedispersed once."""
+    dms = np.arange(0, 8.0, 0.5, dtype=np.float32)
+    buf = _vdif(1.5, seed=21, pulses=[(0.6, 4.0, 2.0, 30.0)])
+    plan, per = _stream_run(vf, dms, [buf])
+    # stream mode uses every complete row (no bundle granularity): one-row bundles
+    L = O.Layout(nave=2, muoslowfreq=384.0, nbundle=1)
+    rows = _oracle_rows(O, co, buf, L)
+    nbp = (rows.shape[0] // 128) * 128
+    bp = co.bandpass(rows[:nbp])
+    off, _ = O.delay_table(dms, L.fch1, L.chanbw, L.tchan, L.nchanout)
+    md = int(off.max())
+    dd = co.dedisperse_cm(co.transpose(bp), off, nbp - md)
+    got = np.concatenate([r["dd"] for r in per[0]], axis=1)
+    n = min(got.shape[1], dd.shape[1])
+    assert n >= dd.shape[1] - 128
+    _close(got[:, :n], dd[:, :n], 5e-5, "stream dedispersed")
+    assert [r["row0"] for r in per[0]] == sorted(r["row0"] for r in per[0])
+
+
+def test_stream_split_invariance_and_isolation(vf):
+    """Results do not depend on how the input is cut, nor on other streams."""
+    dms = np.arange(0, 6.0, 0.5, dtype=np.float32)
+    bufs = [_vdif(0.9, seed=100 + i) for i in range(3)]
+    _, alone = _stream_run(vf, dms, [bufs[1]])
+    _, mixed = _stream_run(vf, dms, bufs, splits=lambda rng: int(rng.integers(1, 400000)))
+    a = np.concatenate([r["dd"] for r in alone[0]], axis=1)
+    m = np.concatenate([r["dd"] for r in mixed[1]], axis=1)
+    assert a.shape == m.shape and np.array_equal(a, m)
+    for s in range(3):
+        assert all(r["device_errors"] == 0 for r in mixed[s])
+
+
+def test_stream_fp16_form(vf):
+    """FP16 storage: series within 3e-3 rms of FP32, identical candidates."""
+    dms = np.arange(0, 12.0, 0.25, dtype=np.float32)
+    buf = _vdif(1.5, seed=31, pulses=[(0.5, 5.0, 2.0, 40.0)])
+    _, f32 = _stream_run(vf, dms, [buf], storage=0)
+    _, f16 = _stream_run(vf, dms, [buf], storage=1)
+    a = np.concatenate([r["dd"] for r in f32[0]], axis=1)
+    b = np.concatenate([r["dd"] for r in f16[0]], axis=1)
+    e = np.max(np.abs(a - b)) / np.sqrt(np.mean(a ** 2))
+    print("fp16 vs fp32 err/rms", e)
+    assert e <= 3e-3
+    ca = [(c["dm_index"], c["t"]) for r in f32[0] for c in r["cands"]]
+    cb = [(c["dm_index"], c["t"]) for r in f16[0] for c in r["cands"]]
+    assert ca == cb and len(ca) >= 1
+    sa = [c["snr"] for r in f32[0] for c in r["cands"]]
+    sb = [c["snr"] for r in f16[0] for c in r["cands"]]
+    assert np.max(np.abs(np.array(sa) - np.array(sb)) / np.array(sa)) <= 0.01

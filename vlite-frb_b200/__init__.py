@@ -271,3 +271,149 @@ def fb_to_time_major(fb_cm, nrows=None, row0=0, row_mask=0xFFFFFFFF, out=None, s
     _check(_lib.vfrb_fb_to_time_major(fb_cm.data_ptr(), fb_cm.stride(0), row0, row_mask, nchan, nrows,
                                       out.data_ptr(), out.stride(0), _stream(stream)), "vfrb_fb_to_time_major")
     return out
+
+
+# ---- plan / stream API -------------------------------------------------------------
+MODE_BLOCK, MODE_STREAM = 0, 1
+READER_PIPE, READER_TS = 0, 1
+OUT_DEDISP, OUT_DMSTATS, OUT_SIGMA, OUT_CHANSTATS, OUT_FB, OUT_CANDS = 1, 2, 4, 8, 16, 32
+VFRB_PENDING = 9
+
+
+class Params(C.Structure):
+    _fields_ = [("twonchan", C.c_int32), ("nave", C.c_int32), ("nbundle", C.c_int32), ("muoslowfreq", C.c_double),
+                ("nchanout_fixed", C.c_int32), ("maxtime", C.c_float), ("timestats", C.c_float),
+                ("dms", C.c_void_p), ("ndm", C.c_int32), ("mode", C.c_int32), ("reader", C.c_int32),
+                ("dada_skip", C.c_int32), ("storage", C.c_int32), ("q_scale", C.c_float), ("outputs", C.c_int32),
+                ("fb_block", C.c_int32), ("nstreams", C.c_int32), ("chunk_seconds", C.c_float),
+                ("ring_seconds", C.c_float), ("cand_snr", C.c_float), ("device", C.c_int32),
+                ("device_bytes", C.c_int64)]
+
+
+class Cand(C.Structure):
+    _fields_ = [("dm_index", C.c_int32), ("width", C.c_int32), ("t", C.c_int64), ("snr", C.c_float),
+                ("dm", C.c_float)]
+
+
+class Result(C.Structure):
+    _fields_ = [("stream", C.c_int32), ("seq", C.c_int64), ("row0", C.c_int64), ("tstart_mjd", C.c_double),
+                ("ndm", C.c_int32), ("nt", C.c_int64), ("dd", C.c_void_p), ("dd_sigma", C.c_void_p),
+                ("ave", C.c_void_p), ("sigma", C.c_void_p), ("peak", C.c_void_p), ("frb", C.c_void_p),
+                ("argmax", C.c_void_p), ("nchan", C.c_int32), ("fb_rows", C.c_int64), ("fb", C.c_void_p),
+                ("nstatblks", C.c_int32), ("chan_ave", C.c_void_p), ("chan_sig", C.c_void_p),
+                ("chan_outlier", C.c_void_p), ("ncand", C.c_int32), ("cands", C.c_void_p),
+                ("latency_ms", C.c_double), ("device_errors", C.c_int32)]
+
+
+_lib.vfrb_params_default.argtypes = [C.POINTER(Params)]
+_lib.vfrb_plan_create.argtypes = [C.POINTER(C.c_void_p), C.POINTER(Params)]
+_lib.vfrb_plan_destroy.argtypes = [C.c_void_p]
+_lib.vfrb_plan_layout.argtypes = [C.c_void_p, C.POINTER(Layout), C.POINTER(C.c_int32)]
+_lib.vfrb_plan_device_bytes.restype = C.c_int64
+_lib.vfrb_plan_device_bytes.argtypes = [C.c_void_p]
+_lib.vfrb_push_frames.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_size_t]
+_lib.vfrb_poll.argtypes = [C.c_void_p, C.POINTER(Result), C.c_int]
+_lib.vfrb_stream_log.restype = C.c_char_p
+_lib.vfrb_stream_log.argtypes = [C.c_void_p, C.c_int]
+
+
+def _arr(ptr, n, dt):
+    if not ptr or n <= 0:
+        return None
+    return np.ctypeslib.as_array(C.cast(ptr, C.POINTER(dt)), shape=(n,)).copy()
+
+
+class Plan:
+    """vfrb_plan: push raw VDIF bytes per stream, poll results (host copies)."""
+
+    def __init__(self, dms=None, **kw):
+        p = Params()
+        _lib.vfrb_params_default(C.byref(p))
+        self._dms = None
+        if dms is not None:
+            self._dms = np.ascontiguousarray(dms, dtype=np.float32)
+            p.dms = self._dms.ctypes.data
+            p.ndm = len(self._dms)
+        for k, v in kw.items():
+            if not hasattr(p, k):
+                raise TypeError(f"unknown parameter {k}")
+            setattr(p, k, v)
+        self.params = p
+        h = C.c_void_p()
+        _check(_lib.vfrb_plan_create(C.byref(h), C.byref(p)), "vfrb_plan_create")
+        self._h = h
+        self.layout = Layout()
+        md = C.c_int32(0)
+        _check(_lib.vfrb_plan_layout(h, C.byref(self.layout), C.byref(md)), "vfrb_plan_layout")
+        self.max_delay = md.value
+
+    @property
+    def device_bytes(self):
+        return int(_lib.vfrb_plan_device_bytes(self._h))
+
+    def push(self, stream: int, data):
+        """data: bytes / numpy uint8 / torch uint8 CPU tensor (pinned or not); None = end of data."""
+        if data is None:
+            _check(_lib.vfrb_push_frames(self._h, stream, None, 0), "vfrb_push_frames")
+            return
+        if hasattr(data, "data_ptr"):
+            ptr, n = data.data_ptr(), data.numel()
+        else:
+            a = np.ascontiguousarray(np.frombuffer(data, np.uint8) if isinstance(data, (bytes, bytearray)) else data)
+            ptr, n = a.ctypes.data, a.nbytes
+            self._keep = a
+        _check(_lib.vfrb_push_frames(self._h, stream, C.c_void_p(ptr), n), "vfrb_push_frames")
+
+    def poll(self, wait=True, copy=True):
+        r = Result()
+        st = _lib.vfrb_poll(self._h, C.byref(r), 1 if wait else 0)
+        if st in (VFRB_EOD, VFRB_PENDING):
+            return None
+        _check(st, "vfrb_poll")
+        if not copy:
+            return r
+        ndm, nt, nch = r.ndm, r.nt, r.nchan
+        out = dict(stream=r.stream, seq=r.seq, row0=r.row0, tstart_mjd=r.tstart_mjd, ndm=ndm, nt=nt,
+                   latency_ms=r.latency_ms, device_errors=r.device_errors)
+        dd = _arr(r.dd, ndm * nt, C.c_float)
+        out["dd"] = dd.reshape(ndm, nt) if dd is not None else None
+        ds = _arr(r.dd_sigma, ndm * nt, C.c_float)
+        out["dd_sigma"] = ds.reshape(ndm, nt) if ds is not None else None
+        for k, dt in (("ave", C.c_float), ("sigma", C.c_float), ("peak", C.c_float), ("frb", C.c_int32),
+                      ("argmax", C.c_int32)):
+            out[k] = _arr(getattr(r, k), ndm, dt)
+        fb = _arr(r.fb, r.fb_rows * nch, C.c_float)
+        out["fb"] = fb.reshape(r.fb_rows, nch) if fb is not None else None
+        for k in ("chan_ave", "chan_sig", "chan_outlier"):
+            a = _arr(getattr(r, k), r.nstatblks * nch, C.c_float)
+            out[k] = a.reshape(r.nstatblks, nch) if a is not None else None
+        cands = []
+        if r.ncand and r.cands:
+            ca = C.cast(r.cands, C.POINTER(Cand))
+            for i in range(r.ncand):
+                c = ca[i]
+                cands.append(dict(dm_index=c.dm_index, width=c.width, t=c.t, snr=c.snr, dm=c.dm))
+        out["cands"] = cands
+        return out
+
+    def drain(self):
+        res = []
+        while True:
+            r = self.poll(wait=True)
+            if r is None:
+                return res
+            res.append(r)
+
+    def log(self, stream=0) -> str:
+        return _lib.vfrb_stream_log(self._h, stream).decode()
+
+    def close(self):
+        if getattr(self, "_h", None):
+            _lib.vfrb_plan_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

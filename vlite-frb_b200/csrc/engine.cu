@@ -603,7 +603,10 @@ int64_t oldest_ref(const StreamSt* s) {
 
 // Copy `nf` whole frames to the ring, queue their headers, advance.
 int feed_frames(vfrb_plan* pl, StreamSt* s, const uint8_t* host, int64_t nf, bool pinned) {
-  const int64_t batch_max = std::max<int64_t>(1, std::min<int64_t>(s->ring_frames / 4, (int64_t)s->stage_frames));
+  // page-locked input is copied in place, in quarters of the ring; other
+  // input goes through the (smaller) staging buffers
+  const int64_t batch_max =
+      std::max<int64_t>(1, pinned ? s->ring_frames / 4 : std::min<int64_t>(s->ring_frames / 4, (int64_t)s->stage_frames));
   for (int64_t done = 0; done < nf;) {
     const int64_t nb = std::min(batch_max, nf - done);
     const uint8_t* src = host + done * kFrameLen;
