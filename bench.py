@@ -152,14 +152,16 @@ class DevicePipeline:
         self.ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
         self.t_k = [0.0, 0.0, 0.0]
         self.n_timed = 0
+        self.uscale = 0.0
         if storage != 0:
-            # per-channel scale from the first window's variance (the running bandpass state)
+            # FP16 form: one scale per stream from the first window's variance
             vf.channelise(frames, self.s0, self.s1, 0, 128, self.L, out=self.raw)
             var = torch.empty((1, nch), device=dev)
             vf.bandpass(self.raw, nrows=128, win_var=var)
-            s = torch.sqrt(torch.clamp(var[0], min=1e-30))
-            self.scale = s
-            self.inv = 1.0 / s
+            S = float(torch.sqrt(torch.clamp(var[0], min=0).mean()).item())
+            self.uscale = S
+            self.inv = torch.full((nch,), 1.0 / S, device=dev)
+        self.tune = self.plan.autotune(storage, self.rows)
 
     def step(self, timed=False):
         vf, torch = self.vf, self.torch
@@ -179,7 +181,7 @@ class DevicePipeline:
             row0, nt = 0, self.rows - self.md
         else:
             row0, nt = r0 - self.md, self.rows
-        out, st = self.plan(self.ring, nt, storage=self.storage, chan_scale=self.scale, row0=row0,
+        out, st = self.plan(self.ring, nt, storage=self.storage, uniform_scale=self.uscale, row0=row0,
                             row_mask=self.R - 1, nrows_valid=nt + self.md, out=self.out, workspace=self.ws)
         self.stats = st
         if timed:
@@ -216,7 +218,8 @@ def run_device(vf, frames, storage, steps, warmup, dist):
     ms = dist_max(dist, ms)
     stage /= steps
     return dict(ms=ms, stage_ms=stage.tolist(), rows=pipe.rows, md=pipe.md, clocks=clk.summary(),
-                stats=pipe.stats, nchan=pipe.L.nchanout, launches=4)
+                stats=pipe.stats, nchan=pipe.L.nchanout, launches=4, tune=pipe.tune,
+                variant=pipe.plan.variant(storage))
 
 
 # --------------------------------------------------------------------------- e2e through the plan API
@@ -515,12 +518,14 @@ def main():
         "latency_ms": {"p50": float(np.nanpercentile(lat, 50)), "p99": float(np.nanpercentile(lat, 99)),
                        "chunk_ms": 1000.0, "n": int(len(lat))},
         "gpu_launches": f32["launches"] * args.steps,
+        "dedisperse_autotune_ms": {"variant": f32["variant"], "times": {str(k): v for k, v in f32["tune"].items()}},
         "gen_seconds": t_gen,
     }
     if f16 is not None:
         line["fp16"] = {"value": world * data_s / (f16["ms"] / 1000.0), "ms_per_step": f16["ms"],
                         "stages_ms_per_step": f16["stage_ms"], "speedup_vs_f32": f32["ms"] / f16["ms"],
-                        "dedisperse_speedup_vs_f32": f32["stage_ms"][2] / f16["stage_ms"][2]}
+                        "dedisperse_speedup_vs_f32": f32["stage_ms"][2] / f16["stage_ms"][2],
+                        "autotune_ms": {"variant": f16["variant"], "times": {str(k): v for k, v in f16["tune"].items()}}}
     if not args.skip_extras:
         try:
             line["cpu_baseline"] = {k: v for k, v in cpu_baseline(args.cpu_sample).items() if k != "seconds"}

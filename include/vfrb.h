@@ -151,10 +151,26 @@ int vfrb_ddplan_max_delay(const vfrb_ddplan* plan);
  * staged/direct kernels apply (no reference counterpart; introspection). */
 int vfrb_ddplan_group_size(const vfrb_ddplan* plan);
 
+/* Kernel variants of the dedisperser (no reference counterpart).  AUTO uses
+ * the autotuned choice (or the largest register group that fits). */
+#define VFRB_DD_AUTO 0
+#define VFRB_DD_STAGED 1   /* shared-memory tile, one load per add           */
+#define VFRB_DD_REG1 2     /* register window, 1 trial per thread            */
+#define VFRB_DD_REG2 3     /* register window, 2 adjacent trials per thread  */
+#define VFRB_DD_REG4 4     /* register window, 4 adjacent trials per thread  */
+#define VFRB_DD_DIRECT 5   /* direct loads (delay spreads too wide to stage) */
+int vfrb_ddplan_set_variant(vfrb_ddplan* plan, int storage, int variant);
+int vfrb_ddplan_variant(const vfrb_ddplan* plan, int storage);
+/* Times every applicable variant on scratch data of the given shape
+ * (nt_out samples per trial, `storage` form) and keeps the fastest.  Writes
+ * the per-variant times in ms to times[6] (index = variant, < 0 = n/a). */
+int vfrb_ddplan_autotune(vfrb_ddplan* plan, int storage, int64_t nt_out, float* times, void* stream);
+
 typedef struct vfrb_dd_args {
   const void* fb;            /* device: channel-major FB in `storage` form       */
   int32_t storage;
   const float* chan_scale;   /* device [nchan]: w_c for F16/I8, NULL for F32     */
+  float uniform_scale;       /* F16/I8 with chan_scale NULL: one w for all c     */
   int64_t chan_stride;
   int64_t row0;              /* ring row of output sample 0                      */
   uint32_t row_mask;

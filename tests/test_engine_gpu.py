@@ -76,8 +76,8 @@ def test_block_mode_pipe_chain(vf, O, co):
 def test_block_mode_ts_chain(vf, O, co):
     """TS semantics: 3840 channels, DM {0, 119.3}, dedisperseSTATS sigma."""
     dms = np.array([0.0, 119.3], np.float32)
-    nave, maxtime = 1, 0.4
-    buf = _vdif(1.6, seed=5)
+    nave, maxtime = 4, 1.5  # MAXTIME must exceed the 1.0 s DM-119.3 sweep (TS:442)
+    buf = _vdif(3.1, seed=5)
     plan = vf.Plan(dms, nave=nave, nchanout_fixed=3840, maxtime=maxtime, mode=vf.MODE_BLOCK,
                    reader=vf.READER_TS, outputs=vf.OUT_DEDISP | vf.OUT_SIGMA)
     plan.push(0, buf)

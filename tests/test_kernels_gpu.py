@@ -208,18 +208,15 @@ def test_dedisperse_and_calcstats_match_fp64(vf, O):
     assert np.array_equal(st["argmax"].cpu().numpy(), st_ref["argmax"])
 
 
-@pytest.mark.parametrize("dm_max,ndm,group,force_v1", [
-    (8.0, 70, 4, False), (30.0, 40, 2, False), (120.0, 33, 1, False), (30.0, 40, 2, True)])
-@pytest.mark.parametrize("storage", [0, 1])
-def test_dedisperse_kernel_variants(vf, O, monkeypatch, dm_max, ndm, group, force_v1, storage):
-    """Every register-group size (4, 2, 1 trials per thread) and the staged v1
-    kernel, FP32 and FP16 storage, against the FP64 oracle."""
+@pytest.mark.parametrize("dm_max,ndm,group", [(8.0, 70, 4), (30.0, 40, 2), (120.0, 33, 1)])
+@pytest.mark.parametrize("storage,scaled", [(0, False), (1, False), (1, True)])
+def test_dedisperse_kernel_variants(vf, O, dm_max, ndm, group, storage, scaled):
+    """Every applicable kernel variant (register groups of 4/2/1 trials, the
+    staged and the direct kernel), FP32 and FP16 storage (one scale for all
+    channels, or per-channel weights), against the FP64 oracle."""
     torch = _torch()
-    if force_v1:
-        monkeypatch.setenv("VFRB_DD_V1", "1")
     dms, off, md, fb = _dd_case(ndm=ndm, nch=320, nt=1500, seed=ndm, dm_max=dm_max)
     nt = 1500
-    ref = O.dedisperse(fb.astype(np.float64), off, nt)
     plan = vf.DedispPlan(off)
     assert plan.group_size == group
     dev = torch.device("cuda")
@@ -228,19 +225,28 @@ def test_dedisperse_kernel_variants(vf, O, monkeypatch, dm_max, ndm, group, forc
     cm = np.zeros((fb.shape[1], rows_al), np.float32)
     cm[:, :rows] = fb.T
     x = torch.from_numpy(cm).to(dev)
-    sc = None
+    kw = {}
+    ref = O.dedisperse(fb.astype(np.float64), off, nt)
     if storage == 1:
         x = x.half()
-        sc = torch.ones(fb.shape[1], device=dev)
-        ref = O.dedisperse(cm.T.astype(np.float16).astype(np.float64), off, nt)
-    out, st = plan(x, nt, storage=storage, chan_scale=sc, nrows_valid=rows)
-    torch.cuda.synchronize()
-    rms = np.sqrt(np.mean(ref ** 2))
-    e = np.max(np.abs(out.cpu().numpy() - ref)) / rms
-    print(f"group {group} v1={force_v1} storage={storage}: err/rms {e:.2e}")
-    assert e <= 1e-5
+        ref = O.dedisperse(cm.T.astype(np.float16).astype(np.float64), off, nt) * 0.5
+        kw = dict(chan_scale=torch.full((fb.shape[1],), 0.5, device=dev)) if scaled else dict(uniform_scale=0.5)
     st_ref = O.calcstats_dm(ref)
-    assert np.array_equal(st["frb"].cpu().numpy(), st_ref["frb"])
+    rms = np.sqrt(np.mean(ref ** 2))
+    variants = [vf.DD_STAGED, vf.DD_DIRECT] + [{4: vf.DD_REG4, 2: vf.DD_REG2, 1: vf.DD_REG1}[g]
+                                              for g in (4, 2, 1) if g <= group or g == group]
+    for v in sorted(set(variants)):
+        plan.set_variant(storage, v)
+        out, st = plan(x, nt, storage=storage, nrows_valid=rows, **kw)
+        torch.cuda.synchronize()
+        e = np.max(np.abs(out.cpu().numpy() - ref)) / rms
+        print(f"group {group} variant {v} storage={storage} scaled={scaled}: err/rms {e:.2e}")
+        assert e <= 1e-5, (v, e)
+        assert np.array_equal(st["frb"].cpu().numpy(), st_ref["frb"]), v
+        assert np.allclose(st["peak"].cpu().numpy(), st_ref["peak"], rtol=1e-4), v
+    times = plan.autotune(storage, nt)
+    assert plan.variant(storage) in times and len(times) >= 2
+    print("autotune", times, "->", plan.variant(storage))
 
 
 def test_dedisperse_wide_spread_uses_direct_path(vf, O):

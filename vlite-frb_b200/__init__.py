@@ -18,6 +18,7 @@ LIB_PATH = os.path.join(_HERE, "lib", "libvfrb.so")
 
 VFRB_OK, VFRB_EOD, VFRB_ERR = 0, 1, 2
 F32, F16, I8 = 0, 1, 2
+DD_AUTO, DD_STAGED, DD_REG1, DD_REG2, DD_REG4, DD_DIRECT = 0, 1, 2, 3, 4, 5
 
 
 class VfrbError(RuntimeError):
@@ -75,7 +76,7 @@ class BpArgs(C.Structure):
 
 class DdArgs(C.Structure):
     _fields_ = [("fb", C.c_void_p), ("storage", C.c_int32), ("chan_scale", C.c_void_p),
-                ("chan_stride", C.c_int64), ("row0", C.c_int64), ("row_mask", C.c_uint32),
+                ("uniform_scale", C.c_float), ("chan_stride", C.c_int64), ("row0", C.c_int64), ("row_mask", C.c_uint32),
                 ("nrows_valid", C.c_int64), ("nt_out", C.c_int64), ("out", C.c_void_p), ("out_stride", C.c_int64),
                 ("sigma_out", C.c_void_p), ("workspace", C.c_void_p), ("workspace_bytes", C.c_size_t),
                 ("ave", C.c_void_p), ("sigma", C.c_void_p), ("peak", C.c_void_p), ("frb", C.c_void_p),
@@ -101,6 +102,9 @@ _lib.vfrb_ddplan_create.argtypes = [C.POINTER(C.c_void_p), C.c_void_p, C.c_int, 
 _lib.vfrb_ddplan_destroy.argtypes = [C.c_void_p]
 _lib.vfrb_ddplan_max_delay.argtypes = [C.c_void_p]
 _lib.vfrb_ddplan_group_size.argtypes = [C.c_void_p]
+_lib.vfrb_ddplan_set_variant.argtypes = [C.c_void_p, C.c_int, C.c_int]
+_lib.vfrb_ddplan_variant.argtypes = [C.c_void_p, C.c_int]
+_lib.vfrb_ddplan_autotune.argtypes = [C.c_void_p, C.c_int, C.c_int64, C.c_void_p, C.c_void_p]
 _lib.vfrb_dedisperse_workspace_bytes.restype = C.c_size_t
 _lib.vfrb_dedisperse_workspace_bytes.argtypes = [C.c_void_p, C.c_int64]
 _lib.vfrb_dedisperse.argtypes = [C.c_void_p, C.POINTER(DdArgs), C.c_void_p]
@@ -211,10 +215,22 @@ class DedispPlan:
         self.max_delay = _lib.vfrb_ddplan_max_delay(p)
         self.group_size = _lib.vfrb_ddplan_group_size(p)
 
+    def set_variant(self, storage: int, variant: int):
+        _check(_lib.vfrb_ddplan_set_variant(self._p, storage, variant), "vfrb_ddplan_set_variant")
+
+    def variant(self, storage: int = F32) -> int:
+        return int(_lib.vfrb_ddplan_variant(self._p, storage))
+
+    def autotune(self, storage: int, nt_out: int, stream=None):
+        """Times each applicable kernel variant; returns {variant: ms} (n/a omitted)."""
+        t = (C.c_float * 6)()
+        _check(_lib.vfrb_ddplan_autotune(self._p, storage, nt_out, t, _stream(stream)), "vfrb_ddplan_autotune")
+        return {i: t[i] for i in range(1, 6) if t[i] >= 0}
+
     def workspace_bytes(self, nt_out: int) -> int:
         return int(_lib.vfrb_dedisperse_workspace_bytes(self._p, nt_out))
 
-    def __call__(self, fb_cm, nt_out: int, storage=F32, chan_scale=None, row0=0, row_mask=0xFFFFFFFF,
+    def __call__(self, fb_cm, nt_out: int, storage=F32, chan_scale=None, uniform_scale=0.0, row0=0, row_mask=0xFFFFFFFF,
                  nrows_valid=None, out=None, sigma_out=None, stats=True, workspace=None, d_err=None, stream=None):
         torch = _torch()
         dev = fb_cm.device
@@ -229,7 +245,8 @@ class DedispPlan:
                       argmax=torch.empty(self.ndm, dtype=torch.int32, device=dev))
             if workspace is None:
                 workspace = torch.empty(max(1, self.workspace_bytes(nt_out)), dtype=torch.uint8, device=dev)
-        a = DdArgs(fb=fb_cm.data_ptr(), storage=storage, chan_scale=_ptr(chan_scale), chan_stride=fb_cm.stride(0),
+        a = DdArgs(fb=fb_cm.data_ptr(), storage=storage, chan_scale=_ptr(chan_scale), uniform_scale=uniform_scale,
+                   chan_stride=fb_cm.stride(0),
                    row0=row0, row_mask=row_mask,
                    nrows_valid=fb_cm.shape[1] if nrows_valid is None else nrows_valid, nt_out=nt_out,
                    out=out.data_ptr(), out_stride=out.stride(0), sigma_out=_ptr(sigma_out),

@@ -39,6 +39,7 @@ struct DmPartial {
 struct DdKParams {
   const void* fb;
   const float* chan_scale;
+  float uniform_scale;  // weight of every channel when chan_scale is NULL (F16/I8)
   long long chan_stride;
   long long row0;
   unsigned row_mask;
@@ -117,7 +118,7 @@ __global__ void __launch_bounds__(kDdThreads) k_dedisperse(const DdKParams p) {
       const long long a0 = (p.row0 + t0 + mn) & ~(long long)(VEC - 1);
       if (p.row0 + t0 + mx + kDdNt - a0 > p.lmax) err |= kErrOffsetRange;
       s_abs[cl] = a0;
-      s_w[cl] = (p.chan_scale && cl < nc) ? p.chan_scale[c0 + cl] : 1.f;
+      s_w[cl] = (p.chan_scale && cl < nc) ? p.chan_scale[c0 + cl] : p.uniform_scale;
     }
     __syncthreads();
     // stage rows [s_abs, s_abs + lmax) of each channel of the chunk
@@ -292,7 +293,7 @@ __global__ void __launch_bounds__(256) k_dedisperse_direct(const DdKParams p) {
       const unsigned long long rr = (unsigned long long)(p.row0 + t + o) & (unsigned long long)p.row_mask;
       const float v = to_f<T>(fb[(long long)c * p.chan_stride + rr]);
       if (sizeof(T) == 4) acc += v;
-      else acc = fmaf(p.chan_scale[c], v, acc);
+      else acc = fmaf(p.chan_scale ? p.chan_scale[c] : p.uniform_scale, v, acc);
       if (SIGMA) acc2 = fmaf(v, v, acc2);
     }
     const float val = acc / (float)p.nchan;
@@ -349,41 +350,64 @@ __global__ void __launch_bounds__(256) k_dedisperse_direct(const DdKParams p) {
 
 #include "dedisperse_reg.cuh"
 
+
 // ---- plan object --------------------------------------------------------------
-struct vfrb_ddplan {
-  int ndm = 0, nchan = 0;
-  int max_delay = 0;   // max over the table
-  int span16 = 0;      // max over 16-DM blocks and channels of (max - min) delay
-  int* d_off = nullptr;
-  // register-window variant: groups of D adjacent trials, shifts <= smax
-  int reg_d = 0, reg_smax = 0, reg_span = 0, ngroups = 0, nblocks = 0;
+namespace vfrb {
+// Register-window grouping for one group size D: per (group, channel) the
+// group's smallest delay and the D delay differences (8 bits each), and per
+// CTA block of kRegWarps groups the smallest delay (tile start).
+struct RegGroup {
+  int D = 0;
+  int smax = 0;  // largest in-group delay difference
+  int span = 0;  // largest (max - min) delay over a CTA block's trials
+  int ngroups = 0, nblocks = 0;
   int* d_gbase = nullptr;
   unsigned* d_gpack = nullptr;
   int* d_bmin = nullptr;
 };
+}  // namespace vfrb
+
+struct vfrb_ddplan {
+  int ndm = 0, nchan = 0;
+  int max_delay = 0;  // max over the table
+  int span16 = 0;     // max over 16-trial blocks and channels of (max - min) delay
+  int* d_off = nullptr;
+  vfrb::RegGroup reg[3];            // D = 4, 2, 1 when applicable
+  int variant[3] = {0, 0, 0};       // chosen variant per storage form (VFRB_DD_*)
+};
 
 namespace vfrb {
+
+static const RegGroup* find_group(const vfrb_ddplan* pl, int D) {
+  for (const auto& g : pl->reg)
+    if (g.D == D) return &g;
+  return nullptr;
+}
+
+size_t dedisperse_workspace_bytes_plan(const vfrb_ddplan* pl, long long nt_out) {
+  const long long ntb = (nt_out + kDdNt - 1) / kDdNt;  // every kernel's time block is >= 256 samples
+  return (size_t)ntb * (size_t)pl->ndm * sizeof(DmPartial);
+}
 
 static int dd_lmax(const vfrb_ddplan* pl, int vec) {
   const int need = kDdNt + pl->span16 + vec;  // + alignment slack
   return (need + 15) & ~15;
 }
 
-size_t dedisperse_workspace_bytes_plan(const vfrb_ddplan* pl, long long nt_out) {
-  const long long ntb = (nt_out + kDdNt - 1) / kDdNt;
-  return (size_t)ntb * (size_t)pl->ndm * sizeof(DmPartial);
-}
-
+// staged (v1) or direct kernel; returns the number of time blocks in *ntb
 template <typename T, bool SIGMA>
-static int dd_launch_t(const vfrb_ddplan* pl, const vfrb_dd_args& a, DdKParams& k, cudaStream_t s) {
+static int dd_launch_t(const vfrb_ddplan* pl, const vfrb_dd_args& a, DdKParams& k, cudaStream_t s, bool allow_staged,
+                       int* ntb) {
   constexpr int VEC = Vec<T>::n;
   const int lmax = dd_lmax(pl, VEC);
   const size_t fixed = ((size_t)kDdDm * kDdMaxChunk * 4 + kDdMaxChunk * 8 + kDdMaxChunk * 4 + 8 * 4 + 15) / 16 * 16;
   int chunk = (int)((kDdSmemBudget - fixed) / ((size_t)lmax * sizeof(T)));
   chunk = std::min(chunk, kDdMaxChunk);
-  const long long ntb = (a.nt_out + kDdNt - 1) / kDdNt;
-  const bool vec_ok = (a.chan_stride % VEC) == 0 && ((unsigned long long)a.row_mask + 1ULL) % VEC == 0;
-  if (chunk >= 4 && vec_ok) {
+  const long long tb = (a.nt_out + kDdNt - 1) / kDdNt;
+  const bool vec_ok = (a.chan_stride % VEC) == 0 && ((unsigned long long)a.row_mask + 1ULL) % VEC == 0 &&
+                      ((uintptr_t)a.fb & 15) == 0;
+  *ntb = (int)tb;
+  if (allow_staged && chunk >= 4 && vec_ok) {
     k.chunk = chunk;
     k.lmax = lmax;
     const size_t smem = ((size_t)kDdDm * chunk * 4 + chunk * 8 + chunk * 4 + 8 * 4 + 15) / 16 * 16 +
@@ -391,94 +415,101 @@ static int dd_launch_t(const vfrb_ddplan* pl, const vfrb_dd_args& a, DdKParams& 
     cudaError_t e = cudaFuncSetAttribute(k_dedisperse<T, SIGMA>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)smem);
     if (e != cudaSuccess) return VFRB_ERR_CUDA;
-    dim3 grid((unsigned)ntb, (unsigned)((pl->ndm + kDdDm - 1) / kDdDm));
+    dim3 grid((unsigned)tb, (unsigned)((pl->ndm + kDdDm - 1) / kDdDm));
     k_dedisperse<T, SIGMA><<<grid, kDdThreads, smem, s>>>(k);
   } else {
-    dim3 grid((unsigned)ntb, (unsigned)pl->ndm);
+    dim3 grid((unsigned)tb, (unsigned)pl->ndm);
     k_dedisperse_direct<T, SIGMA><<<grid, 256, 0, s>>>(k);
   }
   return cuda_status(cudaGetLastError());
 }
 
 template <typename T, int D, int TT, int SMAX>
-static int reg_launch_t(const vfrb_ddplan* pl, const vfrb_dd_args& a, DmPartial* part, cudaStream_t s, int* ntb) {
+static int reg_launch_t(const vfrb_ddplan* pl, const RegGroup& g, const vfrb_dd_args& a, DmPartial* part,
+                        float out_scale, cudaStream_t s, int* ntb) {
   using Cfg = RegCfg<T, D, TT, SMAX>;
-  const int lmax = (Cfg::NT + pl->reg_span + Cfg::VEC + Cfg::NW + 15) & ~15;
-  const int per_ch = lmax * (int)sizeof(T) * 2 + 2 * (2 * kRegWarps * 4 + 8);
-  int chunk = std::min(32, (int)(96 * 1024 / per_ch));
+  constexpr int VEC = Cfg::VEC;
   *ntb = 0;
-  if (chunk < 2) return VFRB_OK;  // caller falls back (ntb == 0)
+  if (g.D != D || g.smax > SMAX) return VFRB_OK;  // not applicable
+  const int lm = (g.span + 2 * VEC + Cfg::NT + Cfg::NQ * VEC + 32 * VEC + VEC - 1) / VEC * VEC;
+  const int per_ch = 2 * lm * (int)sizeof(T) + 2 * kRegWarps * 16;
+  const int chunk = std::min(32, (int)(96 * 1024 / per_ch));
+  if (chunk < 2) return VFRB_OK;
   DdRegParams k{};
   k.fb = a.fb;
-  k.chan_scale = a.chan_scale;
+  k.out_scale = out_scale;
   k.chan_stride = a.chan_stride;
   k.row0 = a.row0;
   k.row_mask = a.row_mask;
   k.nrows_valid = a.nrows_valid;
   k.nchan = pl->nchan;
   k.ndm = pl->ndm;
-  k.ngroups = pl->ngroups;
+  k.ngroups = g.ngroups;
   k.nt_out = a.nt_out;
   k.out = a.out;
   k.out_stride = a.out_stride;
   k.part = part;
-  k.gbase = pl->d_gbase;
-  k.gpack = pl->d_gpack;
-  k.bmin = pl->d_bmin;
+  k.gbase = g.d_gbase;
+  k.gpack = g.d_gpack;
+  k.bmin = g.d_bmin;
   k.chunk = chunk;
-  k.lmax = lmax;
+  k.lmax = lm;
   k.err = a.d_err;
-  const int meta_words = 2 * kRegWarps * chunk + 2 * chunk;
-  const size_t smem = (size_t)(2 * meta_words * 4 + 15) / 16 * 16 + (size_t)2 * chunk * lmax * sizeof(T);
+  const size_t smem = (size_t)2 * kRegWarps * chunk * 16 + (size_t)2 * chunk * lm * sizeof(T);
   cudaError_t e = cudaFuncSetAttribute(k_dedisp_reg<T, D, TT, SMAX>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)smem);
   if (e != cudaSuccess) return VFRB_ERR_CUDA;
-  dim3 grid((unsigned)((a.nt_out + Cfg::NT - 1) / Cfg::NT), (unsigned)pl->nblocks);
+  dim3 grid((unsigned)((a.nt_out + Cfg::NT - 1) / Cfg::NT), (unsigned)g.nblocks);
   k_dedisp_reg<T, D, TT, SMAX><<<grid, kRegWarps * 32, smem, s>>>(k);
   const int st = cuda_status(cudaGetLastError());
-  if (st == VFRB_OK) *ntb = (int)grid.x;  // time blocks, for the statistics reduction
+  if (st == VFRB_OK) *ntb = (int)grid.x;
   return st;
 }
 
-// Launches the register-window kernel when it applies.  Returns a status;
-// *ntb is the number of time blocks launched, 0 when the variant does not
-// apply (the caller then uses the staged or direct kernel).
-static int reg_launch(const vfrb_ddplan* pl, const vfrb_dd_args& a, DmPartial* part, cudaStream_t s, int* ntb) {
+// Register-window variant `v` for this call; *ntb == 0 when it does not apply.
+static int reg_launch(const vfrb_ddplan* pl, int v, const vfrb_dd_args& a, DmPartial* part, cudaStream_t s,
+                      int* ntb) {
   *ntb = 0;
-  if (pl->reg_d == 0) return VFRB_OK;
   if (((uintptr_t)a.fb & 15) != 0) return VFRB_OK;
+  const int D = v == VFRB_DD_REG4 ? 4 : v == VFRB_DD_REG2 ? 2 : v == VFRB_DD_REG1 ? 1 : 0;
+  const RegGroup* g = find_group(pl, D);
+  if (!g) return VFRB_OK;
   if (a.storage == VFRB_F32) {
     if (a.chan_stride % 4 || ((unsigned long long)a.row_mask + 1ULL) % 4) return VFRB_OK;
-    if (pl->reg_d == 4) return reg_launch_t<float, 4, 15, 20>(pl, a, part, s, ntb);
-    if (pl->reg_d == 2) return reg_launch_t<float, 2, 15, 16>(pl, a, part, s, ntb);
-    return reg_launch_t<float, 1, 15, 0>(pl, a, part, s, ntb);
+    if (D == 4) return reg_launch_t<float, 4, 12, 20>(pl, *g, a, part, 1.f, s, ntb);
+    if (D == 2) return reg_launch_t<float, 2, 20, 16>(pl, *g, a, part, 1.f, s, ntb);
+    return reg_launch_t<float, 1, 20, 0>(pl, *g, a, part, 1.f, s, ntb);
   }
   if (a.storage == VFRB_F16) {
+    // the mixed-precision add takes no per-channel weight: one scale for all channels
+    if (a.chan_scale || !(a.uniform_scale > 0.f)) return VFRB_OK;
     if (a.chan_stride % 8 || ((unsigned long long)a.row_mask + 1ULL) % 8) return VFRB_OK;
-    if (pl->reg_d == 4) return reg_launch_t<__half, 4, 14, 20>(pl, a, part, s, ntb);
-    if (pl->reg_d == 2) return reg_launch_t<__half, 2, 14, 16>(pl, a, part, s, ntb);
-    return reg_launch_t<__half, 1, 14, 0>(pl, a, part, s, ntb);
+    if (D == 4) return reg_launch_t<__half, 4, 8, 20>(pl, *g, a, part, a.uniform_scale, s, ntb);
+    if (D == 2) return reg_launch_t<__half, 2, 24, 16>(pl, *g, a, part, a.uniform_scale, s, ntb);
+    return reg_launch_t<__half, 1, 24, 0>(pl, *g, a, part, a.uniform_scale, s, ntb);
   }
   return VFRB_OK;
 }
 
-int launch_dedisperse_plan(const vfrb_ddplan* pl, const vfrb_dd_args& a, cudaStream_t s) {
-  if (!pl || !a.fb || !a.out) return VFRB_ERR_ARG;
-  if (a.nt_out <= 0) return a.nt_out == 0 ? VFRB_OK : VFRB_ERR_ARG;
-  if (a.nrows_valid < a.nt_out + pl->max_delay) return VFRB_ERR_ARG;
-  if (a.storage != VFRB_F32 && !a.chan_scale) return VFRB_ERR_ARG;
-  if (a.sigma_out && a.storage != VFRB_F32) return VFRB_ERR_UNSUPPORTED;
-  if ((unsigned long long)a.row_mask != 0xffffffffULL) {
-    const unsigned long long r = (unsigned long long)a.row_mask + 1ULL;
-    if ((r & (r - 1)) != 0) return VFRB_ERR_ARG;  // ring sizes are powers of two
-    if ((long long)r < a.nrows_valid) return VFRB_ERR_ARG;
+static int default_variant(const vfrb_ddplan* pl, int storage) {
+  if (storage == VFRB_F32) {
+    if (find_group(pl, 4)) return VFRB_DD_REG4;
+    if (find_group(pl, 2)) return VFRB_DD_REG2;
+    if (find_group(pl, 1)) return VFRB_DD_REG1;
+  } else if (storage == VFRB_F16) {
+    if (find_group(pl, 2)) return VFRB_DD_REG2;
+    if (find_group(pl, 4)) return VFRB_DD_REG4;
+    if (find_group(pl, 1)) return VFRB_DD_REG1;
   }
+  return VFRB_DD_STAGED;
+}
+
+static int launch_variant(const vfrb_ddplan* pl, int v, const vfrb_dd_args& a, cudaStream_t s) {
   const bool want_stats = a.ave || a.sigma || a.peak || a.frb || a.argmax;
-  const size_t ws = dedisperse_workspace_bytes_plan(pl, a.nt_out);
-  if (want_stats && (!a.workspace || a.workspace_bytes < ws)) return VFRB_ERR_ARG;
   DdKParams k{};
   k.fb = a.fb;
   k.chan_scale = a.chan_scale;
+  k.uniform_scale = a.uniform_scale > 0.f ? a.uniform_scale : 1.f;
   k.chan_stride = a.chan_stride;
   k.row0 = a.row0;
   k.row_mask = a.row_mask;
@@ -492,33 +523,217 @@ int launch_dedisperse_plan(const vfrb_ddplan* pl, const vfrb_dd_args& a, cudaStr
   k.sig_out = a.sigma_out;
   k.part = want_stats ? reinterpret_cast<DmPartial*>(a.workspace) : nullptr;
   k.err = a.d_err;
-  int st;
-  if (!a.sigma_out && !getenv("VFRB_DD_V1")) {
-    int ntb = 0;
-    const int rst = reg_launch(pl, a, k.part, s, &ntb);
-    if (rst) return rst;
-    if (ntb > 0) {
-      if (!want_stats) return VFRB_OK;
-      k_dm_stats<<<(pl->ndm + 7) / 8, 256, 0, s>>>(k.part, ntb, pl->ndm, a.nt_out, a.ave, a.sigma, a.peak, a.frb,
-                                                   a.argmax);
-      return cuda_status(cudaGetLastError());
+  int ntb = 0, st = VFRB_OK;
+  if (!a.sigma_out && (v == VFRB_DD_REG1 || v == VFRB_DD_REG2 || v == VFRB_DD_REG4))
+    st = reg_launch(pl, v, a, k.part, s, &ntb);
+  if (st) return st;
+  if (ntb == 0) {
+    const bool staged = v != VFRB_DD_DIRECT;
+    if (a.sigma_out) {
+      st = dd_launch_t<float, true>(pl, a, k, s, staged, &ntb);
+    } else {
+      switch (a.storage) {
+        case VFRB_F32: st = dd_launch_t<float, false>(pl, a, k, s, staged, &ntb); break;
+        case VFRB_F16: st = dd_launch_t<__half, false>(pl, a, k, s, staged, &ntb); break;
+        case VFRB_I8: st = dd_launch_t<int8_t, false>(pl, a, k, s, staged, &ntb); break;
+        default: return VFRB_ERR_ARG;
+      }
     }
+    if (st) return st;
   }
-  if (a.sigma_out) {
-    st = dd_launch_t<float, true>(pl, a, k, s);
-  } else {
-    switch (a.storage) {
-      case VFRB_F32: st = dd_launch_t<float, false>(pl, a, k, s); break;
-      case VFRB_F16: st = dd_launch_t<__half, false>(pl, a, k, s); break;
-      case VFRB_I8: st = dd_launch_t<int8_t, false>(pl, a, k, s); break;
-      default: return VFRB_ERR_ARG;
-    }
-  }
-  if (st || !want_stats) return st;
-  const long long ntb = (a.nt_out + kDdNt - 1) / kDdNt;
-  k_dm_stats<<<(pl->ndm + 7) / 8, 256, 0, s>>>(k.part, (int)ntb, pl->ndm, a.nt_out, a.ave, a.sigma, a.peak, a.frb,
+  if (!want_stats) return VFRB_OK;
+  k_dm_stats<<<(pl->ndm + 7) / 8, 256, 0, s>>>(k.part, ntb, pl->ndm, a.nt_out, a.ave, a.sigma, a.peak, a.frb,
                                                a.argmax);
   return cuda_status(cudaGetLastError());
+}
+
+int launch_dedisperse_plan(const vfrb_ddplan* pl, const vfrb_dd_args& a, cudaStream_t s) {
+  if (!pl || !a.fb || !a.out) return VFRB_ERR_ARG;
+  if (a.nt_out <= 0) return a.nt_out == 0 ? VFRB_OK : VFRB_ERR_ARG;
+  if (a.nrows_valid < a.nt_out + pl->max_delay) return VFRB_ERR_ARG;
+  if (a.storage != VFRB_F32 && !a.chan_scale && !(a.uniform_scale > 0.f)) return VFRB_ERR_ARG;
+  if (a.storage < VFRB_F32 || a.storage > VFRB_I8) return VFRB_ERR_ARG;
+  if (a.sigma_out && a.storage != VFRB_F32) return VFRB_ERR_UNSUPPORTED;
+  if ((unsigned long long)a.row_mask != 0xffffffffULL) {
+    const unsigned long long r = (unsigned long long)a.row_mask + 1ULL;
+    if ((r & (r - 1)) != 0) return VFRB_ERR_ARG;  // ring sizes are powers of two
+    if ((long long)r < a.nrows_valid) return VFRB_ERR_ARG;
+  }
+  const bool want_stats = a.ave || a.sigma || a.peak || a.frb || a.argmax;
+  if (want_stats && (!a.workspace || a.workspace_bytes < dedisperse_workspace_bytes_plan(pl, a.nt_out)))
+    return VFRB_ERR_ARG;
+  int v = pl->variant[a.storage];
+  if (v == VFRB_DD_AUTO) v = default_variant(pl, a.storage);
+  if (getenv("VFRB_DD_V1")) v = VFRB_DD_STAGED;
+  return launch_variant(pl, v, a, s);
+}
+
+// Time every applicable variant on scratch data and keep the fastest.
+int ddplan_autotune(vfrb_ddplan* pl, int storage, long long nt, float* times, cudaStream_t s) {
+  if (!pl || storage < VFRB_F32 || storage > VFRB_I8 || nt <= 0) return VFRB_ERR_ARG;
+  const size_t eb = storage == VFRB_F32 ? 4 : storage == VFRB_F16 ? 2 : 1;
+  const long long rows = (nt + pl->max_delay + 15) / 16 * 16;
+  void* fb = nullptr;
+  float *out = nullptr, *st = nullptr, *w = nullptr;
+  int* stb = nullptr;
+  void* ws = nullptr;
+  const size_t wsb = dedisperse_workspace_bytes_plan(pl, nt);
+  auto cleanup = [&]() {
+    cudaFree(fb);
+    cudaFree(out);
+    cudaFree(st);
+    cudaFree(stb);
+    cudaFree(ws);
+    cudaFree(w);
+  };
+  if (cudaMalloc(&fb, (size_t)pl->nchan * rows * eb) != cudaSuccess ||
+      cudaMalloc(&out, (size_t)pl->ndm * nt * 4) != cudaSuccess || cudaMalloc(&st, (size_t)pl->ndm * 12) != cudaSuccess ||
+      cudaMalloc(&stb, (size_t)pl->ndm * 8) != cudaSuccess || cudaMalloc(&ws, wsb + 16) != cudaSuccess ||
+      cudaMalloc(&w, (size_t)pl->nchan * 4) != cudaSuccess) {
+    cudaGetLastError();
+    cleanup();
+    return VFRB_ERR_NOMEM;
+  }
+  cudaMemsetAsync(fb, 0, (size_t)pl->nchan * rows * eb, s);
+  cudaMemsetAsync(w, 0, (size_t)pl->nchan * 4, s);
+  vfrb_dd_args a{};
+  a.fb = fb;
+  a.storage = storage;
+  a.chan_scale = storage == VFRB_I8 ? w : nullptr;
+  a.uniform_scale = 1.f;
+  a.chan_stride = rows;
+  a.row_mask = 0xffffffffu;
+  a.nrows_valid = rows;
+  a.nt_out = nt;
+  a.out = out;
+  a.out_stride = nt;
+  a.workspace = ws;
+  a.workspace_bytes = wsb + 16;
+  a.ave = st;
+  a.sigma = st + pl->ndm;
+  a.peak = st + 2 * pl->ndm;
+  a.frb = stb;
+  a.argmax = stb + pl->ndm;
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  float best = 1e30f;
+  int bestv = VFRB_DD_STAGED;
+  for (int v = VFRB_DD_STAGED; v <= VFRB_DD_DIRECT; ++v) {
+    if (times) times[v] = -1.f;
+    if (v == VFRB_DD_DIRECT && bestv != VFRB_DD_STAGED) continue;  // only when nothing faster applies
+    const bool reg = v == VFRB_DD_REG1 || v == VFRB_DD_REG2 || v == VFRB_DD_REG4;
+    if (reg) {
+      const int D = v == VFRB_DD_REG4 ? 4 : v == VFRB_DD_REG2 ? 2 : 1;
+      if (!find_group(pl, D) || storage == VFRB_I8) continue;
+    }
+    if (launch_variant(pl, v, a, s) != VFRB_OK) continue;  // warm-up; also rejects what does not apply
+    cudaEventRecord(e0, s);
+    for (int r = 0; r < 2; ++r) launch_variant(pl, v, a, s);
+    cudaEventRecord(e1, s);
+    if (cudaEventSynchronize(e1) != cudaSuccess) break;
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    ms *= 0.5f;
+    if (times) times[v] = ms;
+    if (ms < best) {
+      best = ms;
+      bestv = v;
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  const int err = cuda_status(cudaStreamSynchronize(s));
+  cleanup();
+  if (err) return err;
+  pl->variant[storage] = bestv;
+  return VFRB_OK;
+}
+
+int ddplan_set_variant(vfrb_ddplan* pl, int storage, int v) {
+  if (!pl || storage < VFRB_F32 || storage > VFRB_I8 || v < VFRB_DD_AUTO || v > VFRB_DD_DIRECT) return VFRB_ERR_ARG;
+  pl->variant[storage] = v;
+  return VFRB_OK;
+}
+
+int ddplan_variant(const vfrb_ddplan* pl, int storage) {
+  if (!pl || storage < VFRB_F32 || storage > VFRB_I8) return -1;
+  return pl->variant[storage] == VFRB_DD_AUTO ? default_variant(pl, storage) : pl->variant[storage];
+}
+
+static int build_group(vfrb_ddplan* p, const int32_t* h_off, int D, int smax_allowed) {
+  const int ndm = p->ndm, nchan = p->nchan;
+  const int ng = (ndm + D - 1) / D;
+  const int DB = kRegWarps * D;
+  const int nb = (ndm + DB - 1) / DB;
+  auto off = [&](int d, int c) { return (int)h_off[(long long)std::min(d, ndm - 1) * nchan + c]; };
+  std::vector<int> gb((size_t)ng * nchan), bm((size_t)nb * nchan);
+  std::vector<unsigned> gp((size_t)ng * nchan);
+  int smax = 0, span = 0;
+  for (int g = 0; g < ng; ++g)
+    for (int c = 0; c < nchan; ++c) {
+      int mn = 0x7fffffff, mx = 0;
+      for (int j = 0; j < D; ++j) {
+        mn = std::min(mn, off(g * D + j, c));
+        mx = std::max(mx, off(g * D + j, c));
+      }
+      smax = std::max(smax, mx - mn);
+      if (smax > smax_allowed) return VFRB_OK;  // this group size does not apply
+      unsigned pk = 0;
+      for (int j = 0; j < D; ++j) pk |= (unsigned)(off(g * D + j, c) - mn) << (8 * j);
+      gb[(size_t)g * nchan + c] = mn;
+      gp[(size_t)g * nchan + c] = pk;
+    }
+  for (int b = 0; b < nb; ++b)
+    for (int c = 0; c < nchan; ++c) {
+      int mn = 0x7fffffff, mx = 0;
+      for (int d = b * DB; d < std::min(ndm, (b + 1) * DB); ++d) {
+        mn = std::min(mn, off(d, c));
+        mx = std::max(mx, off(d, c));
+      }
+      bm[(size_t)b * nchan + c] = mn;
+      span = std::max(span, mx - mn);
+    }
+  RegGroup* slot = nullptr;
+  for (auto& r : p->reg)
+    if (r.D == 0) {
+      slot = &r;
+      break;
+    }
+  if (!slot) return VFRB_OK;
+  RegGroup g;
+  g.D = D;
+  g.smax = smax;
+  g.span = span;
+  g.ngroups = ng;
+  g.nblocks = nb;
+  bool ok = cudaMalloc(&g.d_gbase, gb.size() * sizeof(int)) == cudaSuccess &&
+            cudaMalloc(&g.d_gpack, gp.size() * sizeof(unsigned)) == cudaSuccess &&
+            cudaMalloc(&g.d_bmin, bm.size() * sizeof(int)) == cudaSuccess;
+  ok = ok && cudaMemcpy(g.d_gbase, gb.data(), gb.size() * sizeof(int), cudaMemcpyHostToDevice) == cudaSuccess &&
+       cudaMemcpy(g.d_gpack, gp.data(), gp.size() * sizeof(unsigned), cudaMemcpyHostToDevice) == cudaSuccess &&
+       cudaMemcpy(g.d_bmin, bm.data(), bm.size() * sizeof(int), cudaMemcpyHostToDevice) == cudaSuccess;
+  if (!ok) {
+    cudaGetLastError();
+    cudaFree(g.d_gbase);
+    cudaFree(g.d_gpack);
+    cudaFree(g.d_bmin);
+    return VFRB_ERR_NOMEM;
+  }
+  *slot = g;
+  return VFRB_OK;
+}
+
+int ddplan_destroy(vfrb_ddplan* p) {
+  if (!p) return VFRB_OK;
+  if (p->d_off) cudaFree(p->d_off);
+  for (auto& g : p->reg) {
+    if (g.d_gbase) cudaFree(g.d_gbase);
+    if (g.d_gpack) cudaFree(g.d_gpack);
+    if (g.d_bmin) cudaFree(g.d_bmin);
+  }
+  delete p;
+  return VFRB_OK;
 }
 
 int ddplan_create(vfrb_ddplan** out, const int32_t* h_off, int ndm, int nchan) {
@@ -534,7 +749,7 @@ int ddplan_create(vfrb_ddplan** out, const int32_t* h_off, int ndm, int nchan) {
     }
     mxd = std::max(mxd, (int)h_off[i]);
   }
-  for (int d0 = 0; d0 < ndm; d0 += kDdDm) {
+  for (int d0 = 0; d0 < ndm; d0 += kDdDm)
     for (int c = 0; c < nchan; ++c) {
       int mn = 0x7fffffff, mx = 0;
       for (int d = d0; d < std::min(ndm, d0 + kDdDm); ++d) {
@@ -543,96 +758,31 @@ int ddplan_create(vfrb_ddplan** out, const int32_t* h_off, int ndm, int nchan) {
       }
       span = std::max(span, mx - mn);
     }
-  }
   p->max_delay = mxd;
   p->span16 = span;
-  // register-window grouping: the largest D in {4, 2, 1} whose in-group shifts fit the kernel
-  for (int D : {4, 2, 1}) {
-    const int smax_allowed = (D == 4) ? 20 : (D == 2) ? 16 : 0;
-    const int ng = (ndm + D - 1) / D;
-    int need = 0;
-    for (int g = 0; g < ng && need <= smax_allowed; ++g)
-      for (int c = 0; c < nchan; ++c) {
-        int mn = 0x7fffffff, mx = 0;
-        for (int j = 0; j < D; ++j) {
-          const int d = std::min(g * D + j, ndm - 1);
-          mn = std::min(mn, (int)h_off[(long long)d * nchan + c]);
-          mx = std::max(mx, (int)h_off[(long long)d * nchan + c]);
-        }
-        need = std::max(need, mx - mn);
-      }
-    if (need > smax_allowed) continue;
-    const int DB = kRegWarps * D;
-    p->reg_d = D;
-    p->reg_smax = smax_allowed;
-    p->ngroups = ng;
-    p->nblocks = (ndm + DB - 1) / DB;
-    std::vector<int> gb((size_t)ng * nchan), bm((size_t)p->nblocks * nchan);
-    std::vector<unsigned> gp((size_t)ng * nchan);
-    int rspan = 0;
-    for (int g = 0; g < ng; ++g)
-      for (int c = 0; c < nchan; ++c) {
-        int mn = 0x7fffffff;
-        for (int j = 0; j < D; ++j) mn = std::min(mn, (int)h_off[(long long)std::min(g * D + j, ndm - 1) * nchan + c]);
-        unsigned pk = 0;
-        for (int j = 0; j < D; ++j)
-          pk |= (unsigned)(h_off[(long long)std::min(g * D + j, ndm - 1) * nchan + c] - mn) << (8 * j);
-        gb[(size_t)g * nchan + c] = mn;
-        gp[(size_t)g * nchan + c] = pk;
-      }
-    for (int b = 0; b < p->nblocks; ++b)
-      for (int c = 0; c < nchan; ++c) {
-        int mn = 0x7fffffff, mx = 0;
-        for (int d = b * DB; d < std::min(ndm, (b + 1) * DB); ++d) {
-          mn = std::min(mn, (int)h_off[(long long)d * nchan + c]);
-          mx = std::max(mx, (int)h_off[(long long)d * nchan + c]);
-        }
-        bm[(size_t)b * nchan + c] = mn;
-        rspan = std::max(rspan, mx - mn);
-      }
-    p->reg_span = rspan;
-    bool ok = cudaMalloc(&p->d_gbase, gb.size() * sizeof(int)) == cudaSuccess &&
-              cudaMalloc(&p->d_gpack, gp.size() * sizeof(unsigned)) == cudaSuccess &&
-              cudaMalloc(&p->d_bmin, bm.size() * sizeof(int)) == cudaSuccess;
-    ok = ok && cudaMemcpy(p->d_gbase, gb.data(), gb.size() * sizeof(int), cudaMemcpyHostToDevice) == cudaSuccess &&
-         cudaMemcpy(p->d_gpack, gp.data(), gp.size() * sizeof(unsigned), cudaMemcpyHostToDevice) == cudaSuccess &&
-         cudaMemcpy(p->d_bmin, bm.data(), bm.size() * sizeof(int), cudaMemcpyHostToDevice) == cudaSuccess;
-    if (!ok) {
-      cudaFree(p->d_gbase);
-      cudaFree(p->d_gpack);
-      cudaFree(p->d_bmin);
-      delete p;
-      return VFRB_ERR_NOMEM;
-    }
-    break;
+  // register-window groups: D = 4 and 2 when their in-group shifts fit, else D = 1
+  int st = build_group(p, h_off, 4, 20);
+  if (!st) st = build_group(p, h_off, 2, 16);
+  if (!st && !find_group(p, 2) && !find_group(p, 4)) st = build_group(p, h_off, 1, 0);
+  if (st) {
+    ddplan_destroy(p);
+    return st;
   }
   const size_t bytes = sizeof(int) * (size_t)ndm * nchan;
-  if (cudaMalloc(&p->d_off, bytes) != cudaSuccess) {
-    delete p;
+  if (cudaMalloc(&p->d_off, bytes) != cudaSuccess ||
+      cudaMemcpy(p->d_off, h_off, bytes, cudaMemcpyHostToDevice) != cudaSuccess) {
+    cudaGetLastError();
+    ddplan_destroy(p);
     return VFRB_ERR_NOMEM;
-  }
-  if (cudaMemcpy(p->d_off, h_off, bytes, cudaMemcpyHostToDevice) != cudaSuccess) {
-    cudaFree(p->d_off);
-    delete p;
-    return VFRB_ERR_CUDA;
   }
   *out = p;
   return VFRB_OK;
 }
 
-int ddplan_destroy(vfrb_ddplan* p) {
-  if (!p) return VFRB_OK;
-  if (p->d_off) cudaFree(p->d_off);
-  if (p->d_gbase) cudaFree(p->d_gbase);
-  if (p->d_gpack) cudaFree(p->d_gpack);
-  if (p->d_bmin) cudaFree(p->d_bmin);
-  delete p;
-  return VFRB_OK;
+int ddplan_max_delay(const vfrb_ddplan* p) { return p->max_delay; }
+int ddplan_reg_group(const vfrb_ddplan* p) {
+  const int v = ddplan_variant(p, VFRB_F32);
+  return v == VFRB_DD_REG4 ? 4 : v == VFRB_DD_REG2 ? 2 : v == VFRB_DD_REG1 ? 1 : 0;
 }
 
-}  // namespace vfrb
-
-namespace vfrb {
-int ddplan_max_delay(const vfrb_ddplan* p) { return p->max_delay; }
-int ddplan_reg_group(const vfrb_ddplan* p) { return p->reg_d; }
 }  // namespace vfrb

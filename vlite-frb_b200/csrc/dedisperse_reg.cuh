@@ -2,19 +2,27 @@
 //
 // Each thread owns D adjacent DM trials (a "group") x TT consecutive output
 // samples.  For every channel it loads ONE window of TT + S samples from the
-// shared-memory tile into registers (S = the largest delay difference inside
-// its group for that channel) and adds it, shifted by each trial's delay
-// difference, into D accumulator rows.  The shift is warp-uniform (it depends
-// only on the group and the channel), so a switch over statically indexed
-// cases keeps the window in registers: one shared-memory word feeds up to D
-// additions, which is what lifts the kernel above the shared-memory
-// bandwidth bound of a one-load-per-add kernel.
+// shared-memory tile into registers with 16-byte loads (S = the largest
+// delay difference inside its group for that channel, plus the 16-byte
+// alignment residual) and adds it, shifted by each trial's delay
+// difference, into D accumulator rows.  The shift depends only on the group
+// and the channel, so it is warp-uniform: a switch over statically indexed
+// cases keeps the window in registers, and one shared-memory word feeds up
+// to D additions.  That lifts the kernel above the shared-memory bandwidth
+// bound of a one-load-per-add kernel.
 //
-// Lanes own consecutive TT-sample runs; TT is odd for 4-byte words (FP32) and
-// twice an odd number for FP16 (7 words), so the 32 window loads of a warp
-// hit 32 different banks.  The tile of a chunk of channels is staged with
-// cp.async (16-byte, zero-filled past the valid rows) into the other half of
-// a double buffer while the current chunk is summed.
+// Lanes own consecutive TT-sample runs with TT/VEC odd (VEC = elements per
+// 16 bytes), so the 16-byte loads of each quarter warp hit distinct banks.
+// The per-(group, channel) metadata -- window start in 16-byte units, the D
+// shifts (8 bits each) and the number of 16-byte loads -- is computed while
+// a chunk of channels is staged, and read back with one broadcast load.  The
+// tile of the next chunk is staged with cp.async (16-byte, zero-filled past
+// the valid rows) into the other half of a double buffer while the current
+// chunk is summed.
+//
+// FP16 form: z = (P - mean)/S with one scale S per stream, accumulated in
+// FP32 with the sm_100 mixed-precision add (add.rn.f32.f16), so no
+// per-element conversion; the result is scaled by S at the end.
 #pragma once
 
 namespace vfrb {
@@ -23,7 +31,7 @@ constexpr int kRegWarps = 8;
 
 struct DdRegParams {
   const void* fb;
-  const float* chan_scale;
+  float out_scale;  // multiplies sum/nchan (1 for FP32, S for FP16)
   long long chan_stride;
   long long row0;
   unsigned row_mask;
@@ -39,7 +47,7 @@ struct DdRegParams {
   const unsigned* gpack;   // [ngroups][nchan] D delay differences, 8 bits each
   const int* bmin;         // [nblocks][nchan] smallest delay of a CTA's DM block
   int chunk;
-  int lmax;
+  int lmax;                // tile row length (elements, multiple of 16 bytes)
   int* err;
 };
 
@@ -50,12 +58,44 @@ __device__ __forceinline__ void cp_async16(void* smem_dst, const void* gsrc, int
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::); }
 
-template <int S, int TT, int NW, bool FMA>
-__device__ __forceinline__ void add_at(float (&acc)[TT], const float (&w)[NW], float wc) {
-#pragma unroll
-  for (int i = 0; i < TT; ++i) {
-    if (FMA) acc[i] = fmaf(wc, w[i + S], acc[i]);
-    else acc[i] += w[i + S];
+// acc += half value (FP32 accumulate, sm_100 mixed-precision add)
+__device__ __forceinline__ float add_h(float acc, unsigned short h) {
+  float r;
+  asm("add.rn.f32.f16 %0, %1, %2;" : "=f"(r) : "h"(h), "f"(acc));
+  return r;
+}
+
+// Window storage: one 32-bit register holds PER elements (1 float or 2 halves).
+template <typename T>
+struct RegWin;
+template <>
+struct RegWin<float> {
+  using W = float;
+  static constexpr int VEC = 4;  // elements per 16 bytes
+  static constexpr int PER = 1;  // elements per register
+  template <int E, int NR>
+  __device__ __forceinline__ static float add(float acc, const W (&w)[NR]) {
+    return acc + w[E];
+  }
+};
+template <>
+struct RegWin<__half> {
+  using W = unsigned;  // a half2 word, low half = earlier sample
+  static constexpr int VEC = 8;
+  static constexpr int PER = 2;
+  template <int E, int NR>
+  __device__ __forceinline__ static float add(float acc, const W (&w)[NR]) {
+    unsigned short lo, hi;
+    asm("mov.b32 {%0,%1}, %2;" : "=h"(lo), "=h"(hi) : "r"(w[E >> 1]));
+    return add_h(acc, (E & 1) ? hi : lo);
+  }
+};
+
+template <typename T, int S, int TT, int NR, int I = 0>
+__device__ __forceinline__ void add_at(float (&acc)[TT], const typename RegWin<T>::W (&w)[NR]) {
+  if constexpr (I < TT) {
+    acc[I] = RegWin<T>::template add<I + S, NR>(acc[I], w);
+    add_at<T, S, TT, NR, I + 1>(acc, w);
   }
 }
 
@@ -63,12 +103,12 @@ __device__ __forceinline__ void add_at(float (&acc)[TT], const float (&w)[NW], f
   X(0) X(1) X(2) X(3) X(4) X(5) X(6) X(7) X(8) X(9) X(10) X(11) X(12) X(13) X(14) X(15) X(16) X(17) X(18) \
       X(19) X(20) X(21) X(22) X(23) X(24) X(25) X(26) X(27) X(28) X(29) X(30) X(31)
 
-template <int TT, int NW, bool FMA>
-__device__ __forceinline__ void add_shift(float (&acc)[TT], const float (&w)[NW], int s, float wc) {
+template <typename T, int TT, int NR>
+__device__ __forceinline__ void add_shift(float (&acc)[TT], const typename RegWin<T>::W (&w)[NR], int s) {
   switch (s) {
-#define VFRB_C(S)                                                  \
-  case S:                                                          \
-    if constexpr (S + TT <= NW) add_at<S, TT, NW, FMA>(acc, w, wc); \
+#define VFRB_C(S)                                                                 \
+  case S:                                                                         \
+    if constexpr (S + TT <= NR * RegWin<T>::PER) add_at<T, S, TT, NR>(acc, w);    \
     break;
     VFRB_CASES_0_31(VFRB_C)
 #undef VFRB_C
@@ -79,26 +119,30 @@ __device__ __forceinline__ void add_shift(float (&acc)[TT], const float (&w)[NW]
 
 template <typename T, int D, int TT, int SMAX>
 struct RegCfg {
-  static constexpr bool HALF = sizeof(T) == 2;
-  static constexpr int VEC = 16 / (int)sizeof(T);
-  static constexpr int NW = TT + SMAX + (HALF ? 2 : 0);  // window length in floats
-  static constexpr int NT = 32 * TT;                     // output samples per CTA
-  static constexpr int DB = kRegWarps * D;               // DM trials per CTA
-  static_assert(NW <= 64, "window too long");
-  static_assert(SMAX + (HALF ? 1 : 0) <= 31, "switch covers shifts 0..31");
+  static constexpr int VEC = RegWin<T>::VEC;
+  static constexpr int SHMAX = SMAX + VEC - 1;                 // largest shift incl. alignment residual
+  static constexpr int NQ = (TT + SHMAX + VEC - 1) / VEC;      // 16-byte loads per window
+  static constexpr int NW = NQ * VEC;                          // window elements
+  static constexpr int NR = NQ * 4;                            // window registers (32-bit)
+  static constexpr int NT = 32 * TT;                           // output samples per CTA
+  static constexpr int DB = kRegWarps * D;                     // DM trials per CTA
+  static_assert(TT % VEC == 0 && ((TT / VEC) & 1) == 1, "lane stride must be an odd number of 16-byte units");
+  static_assert(SHMAX <= 31, "switch covers shifts 0..31");
+  static_assert(D <= 4, "shifts are packed in one 32-bit word");
 };
 
 template <typename T, int D, int TT, int SMAX>
 __global__ void __launch_bounds__(kRegWarps * 32, 2) k_dedisp_reg(const DdRegParams p) {
   using Cfg = RegCfg<T, D, TT, SMAX>;
-  constexpr bool HALF = Cfg::HALF;
-  constexpr int VEC = Cfg::VEC, NW = Cfg::NW, NT = Cfg::NT;
-  extern __shared__ float4 sm4[];
+  using W = typename RegWin<T>::W;
+  static_assert(sizeof(W) == 4, "window registers are 32-bit");
+  constexpr int VEC = Cfg::VEC, NQ = Cfg::NQ, NR = Cfg::NR, NT = Cfg::NT;
+  extern __shared__ int4 smr4[];
   const int CH = p.chunk, LM = p.lmax;
-  // shared layout: meta[2] { int gb[W][CH]; unsigned gp[W][CH]; long long a0[CH] } then tile[2][CH][LM]
-  const int meta_words = 2 * kRegWarps * CH + 2 * CH;  // 4-byte words per buffer
-  int* meta = reinterpret_cast<int*>(sm4);
-  T* tiles = reinterpret_cast<T*>(sm4 + (2 * meta_words * 4 + 15) / 16);
+  const int LMQ = LM / VEC;  // tile row length in 16-byte units
+  // shared layout: meta[2][W][CH] int4 {window start (16-byte units), shifts, loads, 0}, then tile[2][CH][LM]
+  int4* meta = smr4;
+  int4* tiles = smr4 + 2 * kRegWarps * CH;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const long long t0 = (long long)blockIdx.x * NT;
   const int blk = blockIdx.y;
@@ -107,35 +151,44 @@ __global__ void __launch_bounds__(kRegWarps * 32, 2) k_dedisp_reg(const DdRegPar
   const int nchunks = (p.nchan + CH - 1) / CH;
   int err = 0;
 
-  auto gbs = [&](int b) { return meta + b * meta_words; };
-  auto gps = [&](int b) { return reinterpret_cast<unsigned*>(meta + b * meta_words + kRegWarps * CH); };
-  auto a0s = [&](int b) { return reinterpret_cast<long long*>(meta + b * meta_words + 2 * kRegWarps * CH); };
-
   auto stage = [&](int k, int b) {
     const int c0 = k * CH;
     const int nc = min(CH, p.nchan - c0);
-    int* gb = gbs(b);
-    unsigned* gp = gps(b);
-    long long* a0 = a0s(b);
+    int4* mb = meta + b * kRegWarps * CH;
     for (int i = tid; i < kRegWarps * CH; i += kRegWarps * 32) {
       const int w = i / CH, cl = i - w * CH;
       const int g = min(g0 + w, p.ngroups - 1);
       const int c = c0 + min(cl, nc - 1);
-      gb[i] = __ldg(p.gbase + (long long)g * p.nchan + c);
-      gp[i] = __ldg(p.gpack + (long long)g * p.nchan + c);
+      const long long a0 = (p.row0 + t0 + __ldg(p.bmin + (long long)blk * p.nchan + c)) & ~(long long)(VEC - 1);
+      int rel = (int)(p.row0 + t0 + __ldg(p.gbase + (long long)g * p.nchan + c) - a0);
+      const unsigned pk = __ldg(p.gpack + (long long)g * p.nchan + c);
+      const int res = rel & (VEC - 1);
+      unsigned sh = 0;
+      int smx = 0;
+#pragma unroll
+      for (int j = 0; j < D; ++j) {
+        const int s = min((int)((pk >> (8 * j)) & 0xFFu), SMAX) + res;
+        sh |= (unsigned)s << (8 * j);
+        smx = max(smx, s);
+      }
+      int q0 = rel / VEC;
+      if (rel < 0 || (q0 + 31 * (TT / VEC) + NQ) > LMQ) {  // cannot happen with a consistent plan
+        err |= kErrOffsetRange;
+        q0 = 0;
+      }
+      mb[i] = make_int4(q0, (int)sh, (TT + smx + VEC - 1) / VEC, 0);
     }
     for (int cl = warp; cl < nc; cl += kRegWarps) {
       const long long a = (p.row0 + t0 + __ldg(p.bmin + (long long)blk * p.nchan + c0 + cl)) & ~(long long)(VEC - 1);
-      if (lane == 0) a0[cl] = a;
       const T* src = fb + (long long)(c0 + cl) * p.chan_stride;
-      T* dst = tiles + ((long long)b * CH + cl) * LM;
+      int4* dst = tiles + ((long long)b * CH + cl) * LMQ;
       const long long vend = p.row0 + p.nrows_valid;
-      for (int v = lane; v < LM / VEC; v += 32) {
+      for (int v = lane; v < LMQ; v += 32) {
         const long long r = a + (long long)v * VEC;
         int bytes = 0;
         if (r >= 0 && r < vend) bytes = (int)(min((long long)VEC, vend - r) * (long long)sizeof(T));
         const unsigned long long rr = (unsigned long long)(bytes ? r : 0) & (unsigned long long)p.row_mask;
-        cp_async16(dst + (long long)v * VEC, src + rr, bytes);
+        cp_async16(dst + v, src + rr, bytes);
       }
     }
     cp_async_commit();
@@ -153,57 +206,39 @@ __global__ void __launch_bounds__(kRegWarps * 32, 2) k_dedisp_reg(const DdRegPar
     __syncthreads();
     if (k + 1 < nchunks) stage(k + 1, (k + 1) & 1);
     const int b = k & 1;
-    const int c0 = k * CH;
-    const int nc = min(CH, p.nchan - c0);
-    const int* gb = gbs(b) + warp * CH;
-    const unsigned* gp = gps(b) + warp * CH;
-    const long long* a0 = a0s(b);
-    const T* tile = tiles + (long long)b * CH * LM;
+    const int nc = min(CH, p.nchan - k * CH);
+    const int4* mb = meta + (b * kRegWarps + warp) * CH;
+    const int4* tile = tiles + (long long)b * CH * LMQ + lane * (TT / VEC);
+#pragma unroll 1
     for (int cl = 0; cl < nc; ++cl) {
-      const unsigned pk = gp[cl];
-      int sh[D];
-      int smax = 0;
+      const int4 m = mb[cl];
+      const int4* q = tile + (long long)cl * LMQ + m.x;
+      // the whole window, unconditionally: tile rows are padded so every
+      // load stays inside the row, and no register keeps an old value
+      W w[NR];
 #pragma unroll
-      for (int j = 0; j < D; ++j) {
-        sh[j] = min((int)((pk >> (8 * j)) & 0xFFu), SMAX);
-        smax = max(smax, sh[j]);
-      }
-      int start = (int)(p.row0 + t0 + gb[cl] - a0[cl]);
-      if (start < 0 || start + NT + NW > LM) {  // cannot happen with a consistent plan; never read outside the tile
-        err |= kErrOffsetRange;
-        start = min(max(start, 0), LM - NT - NW);
-      }
-      start += lane * TT;
-      const T* trow = tile + (long long)cl * LM;
-      float w[NW];
-      float wc = 1.f;
-      int par = 0;
-      if constexpr (!HALF) {
-#pragma unroll
-        for (int i = 0; i < NW; ++i) w[i] = (i < TT + smax) ? trow[start + i] : 0.f;
-      } else {
-        wc = p.chan_scale[c0 + cl];
-        par = start & 1;
-        const __half2* hw = reinterpret_cast<const __half2*>(trow + (start - par));
-        const int nwords = (TT + smax + par + 1) >> 1;
-#pragma unroll
-        for (int q = 0; q < NW / 2; ++q) {
-          if (q < nwords) {
-            const float2 f = __half22float2(hw[q]);
-            w[2 * q] = f.x;
-            w[2 * q + 1] = f.y;
-          } else {
-            w[2 * q] = 0.f;
-            w[2 * q + 1] = 0.f;
-          }
+      for (int qi = 0; qi < NQ; ++qi) {
+        const int4 v = q[qi];
+        if constexpr (sizeof(W) == 4 && RegWin<T>::PER == 1) {
+          w[4 * qi + 0] = __int_as_float(v.x);
+          w[4 * qi + 1] = __int_as_float(v.y);
+          w[4 * qi + 2] = __int_as_float(v.z);
+          w[4 * qi + 3] = __int_as_float(v.w);
+        } else {
+          w[4 * qi + 0] = (W)v.x;
+          w[4 * qi + 1] = (W)v.y;
+          w[4 * qi + 2] = (W)v.z;
+          w[4 * qi + 3] = (W)v.w;
         }
       }
 #pragma unroll
-      for (int j = 0; j < D; ++j) add_shift<TT, NW, HALF>(acc[j], w, sh[j] + par, wc);
+      for (int j = 0; j < D; ++j) add_shift<T, TT, NR>(acc[j], w, (int)(((unsigned)m.y >> (8 * j)) & 0xFFu));
     }
   }
 
-  // epilogue: out = sum / NCHANOUT (PIPE:1534); calcstats partials per (DM, time block)
+  // epilogue: out = sum / NCHANOUT (PIPE:1534) x scale; calcstats partials per (DM, time block)
+  const float fs = p.out_scale / (float)p.nchan;
+  const bool plain = p.out_scale == 1.f;
   const float fn = (float)p.nchan;
 #pragma unroll
   for (int j = 0; j < D; ++j) {
@@ -217,7 +252,7 @@ __global__ void __launch_bounds__(kRegWarps * 32, 2) k_dedisp_reg(const DdRegPar
     for (int i = 0; i < TT; ++i) {
       const long long t = t0 + (long long)lane * TT + i;
       if (t < p.nt_out) {
-        const float val = acc[j][i] / fn;
+        const float val = plain ? acc[j][i] / fn : acc[j][i] * fs;
         orow[t] = val;
         s += (double)val;
         s2 += (double)val * (double)val;
@@ -239,12 +274,12 @@ __global__ void __launch_bounds__(kRegWarps * 32, 2) k_dedisp_reg(const DdRegPar
       }
     }
     if (lane == 0 && p.part) {
-      DmPartial q;
-      q.s = s;
-      q.s2 = s2;
-      q.mx = mx;
-      q.arg = arg;
-      p.part[(long long)blockIdx.x * p.ndm + d] = q;
+      DmPartial pq;
+      pq.s = s;
+      pq.s2 = s2;
+      pq.mx = mx;
+      pq.arg = arg;
+      p.part[(long long)blockIdx.x * p.ndm + d] = pq;
     }
   }
   if (err && p.err) atomicOr(p.err, err);

@@ -37,6 +37,7 @@ int launch_dedisperse_plan(const vfrb_ddplan* pl, const vfrb_dd_args& a, cudaStr
 int ddplan_create(vfrb_ddplan** out, const int32_t* h_off, int ndm, int nchan);
 int ddplan_destroy(vfrb_ddplan* p);
 int ddplan_max_delay(const vfrb_ddplan* p);
+int ddplan_autotune(vfrb_ddplan* pl, int storage, long long nt, float* times, cudaStream_t s);
 
 static double now_ms() {
   using namespace std::chrono;
@@ -76,6 +77,25 @@ __global__ void k_init_scale(const float* var, int nchan, float q, int storage, 
   if (!(s > 1e-30f)) s = 1.f;
   inv[c] = 1.f / s;
   w[c] = (storage == VFRB_I8) ? s / q : s;
+}
+
+// FP16 form: one scale per stream, S = sqrt(mean_c var_c) of the first
+// window (FP16 keeps its relative precision at any scale; S only keeps the
+// values well inside the FP16 range).  w[0] = S, inv[c] = 1/S.
+__global__ void k_uniform_scale(const float* var, int nchan, float* w, float* inv) {
+  __shared__ double part[256];
+  double s = 0.0;
+  for (int c = threadIdx.x; c < nchan; c += blockDim.x) s += (double)fmaxf(var[c], 0.f);
+  part[threadIdx.x] = s;
+  __syncthreads();
+  for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+    if ((int)threadIdx.x < o) part[threadIdx.x] += part[threadIdx.x + o];
+    __syncthreads();
+  }
+  float S = (float)sqrt(part[0] / (double)nchan);
+  if (!(S > 1e-30f)) S = 1.f;
+  if (threadIdx.x == 0) w[0] = S;
+  for (int c = threadIdx.x; c < nchan; c += blockDim.x) inv[c] = 1.f / S;
 }
 
 struct ResultSlot {
@@ -143,6 +163,7 @@ struct StreamSt {
   unsigned cm_mask = 0xffffffffu;
   float *d_w = nullptr, *d_inv = nullptr, *d_var = nullptr, *d_scr = nullptr;
   bool scale_ready = false;
+  float uscale = 1.f;  // FP16 form: the stream's single scale S
   float *d_out = nullptr, *d_sig = nullptr, *d_ave = nullptr, *d_sgm = nullptr, *d_peak = nullptr;
   int32_t *d_frb = nullptr, *d_arg = nullptr;
   void* d_ws = nullptr;
@@ -363,8 +384,17 @@ int init_scale(vfrb_plan* pl, StreamSt* s, const float* raw, int64_t row0, unsig
   a.win_var = s->d_var;
   ST(launch_bandpass(a, s->cs));
   const int nch = pl->L.nchanout;
-  k_init_scale<<<(nch + 255) / 256, 256, 0, s->cs>>>(s->d_var, nch, pl->P.q_scale, pl->P.storage, s->d_w, s->d_inv);
-  CK(cudaGetLastError());
+  if (pl->P.storage == VFRB_F16) {
+    k_uniform_scale<<<1, 256, 0, s->cs>>>(s->d_var, nch, s->d_w, s->d_inv);
+    CK(cudaGetLastError());
+    // the dedisperser takes S by value: read it once per stream
+    CK(cudaMemcpyAsync(&s->uscale, s->d_w, sizeof(float), cudaMemcpyDeviceToHost, s->cs));
+    CK(cudaStreamSynchronize(s->cs));
+  } else {
+    k_init_scale<<<(nch + 255) / 256, 256, 0, s->cs>>>(s->d_var, nch, pl->P.q_scale, pl->P.storage, s->d_w,
+                                                        s->d_inv);
+    CK(cudaGetLastError());
+  }
   s->scale_ready = true;
   return VFRB_OK;
 }
@@ -397,7 +427,8 @@ int run_dedisp(vfrb_plan* pl, StreamSt* s, int64_t row0, int64_t nrows_valid, in
   vfrb_dd_args a{};
   a.fb = s->d_cm;
   a.storage = pl->P.storage;
-  a.chan_scale = pl->P.storage == VFRB_F32 ? nullptr : s->d_w;
+  a.chan_scale = pl->P.storage == VFRB_I8 ? s->d_w : nullptr;
+  a.uniform_scale = pl->P.storage == VFRB_F16 ? s->uscale : 0.f;
   a.chan_stride = s->cm_stride;
   a.row0 = row0;
   a.row_mask = s->cm_mask;
@@ -857,6 +888,12 @@ int vfrb_plan_create(vfrb_plan** out, const vfrb_params* prm) {
   for (auto& s : pl->st)
     if (cudaStreamSynchronize(s->cs) != cudaSuccess || cudaStreamSynchronize(s->xs) != cudaSuccess)
       return fail(VFRB_ERR_CUDA);
+  if (pl->want_dd && !(P.outputs & VFRB_OUT_SIGMA)) {
+    // pick the fastest dedispersion kernel variant for this grid and chunk
+    const int64_t nt = P.mode == VFRB_MODE_BLOCK ? pl->nt_block : pl->chunk_rows;
+    st = ddplan_autotune(pl->dd, P.storage, nt, nullptr, pl->st[0]->cs);
+    if (st) return fail(st);
+  }
   *out = pl;
   return VFRB_OK;
 }

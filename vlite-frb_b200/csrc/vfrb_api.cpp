@@ -12,6 +12,9 @@ int ddplan_create(vfrb_ddplan** out, const int32_t* h_off, int ndm, int nchan);
 int ddplan_destroy(vfrb_ddplan* p);
 int ddplan_max_delay(const vfrb_ddplan* p);
 int ddplan_reg_group(const vfrb_ddplan* p);
+int ddplan_autotune(vfrb_ddplan* pl, int storage, long long nt, float* times, cudaStream_t s);
+int ddplan_set_variant(vfrb_ddplan* pl, int storage, int v);
+int ddplan_variant(const vfrb_ddplan* pl, int storage);
 }  // namespace vfrb
 
 extern "C" {
@@ -143,6 +146,16 @@ int vfrb_ddplan_destroy(vfrb_ddplan* plan) { return vfrb::ddplan_destroy(plan); 
 int vfrb_ddplan_max_delay(const vfrb_ddplan* plan) { return plan ? vfrb::ddplan_max_delay(plan) : -1; }
 
 int vfrb_ddplan_group_size(const vfrb_ddplan* plan) { return plan ? vfrb::ddplan_reg_group(plan) : -1; }
+
+int vfrb_ddplan_set_variant(vfrb_ddplan* plan, int storage, int variant) {
+  return vfrb::ddplan_set_variant(plan, storage, variant);
+}
+
+int vfrb_ddplan_variant(const vfrb_ddplan* plan, int storage) { return vfrb::ddplan_variant(plan, storage); }
+
+int vfrb_ddplan_autotune(vfrb_ddplan* plan, int storage, int64_t nt_out, float* times, void* stream) {
+  return vfrb::ddplan_autotune(plan, storage, nt_out, times, (cudaStream_t)stream);
+}
 
 size_t vfrb_dedisperse_workspace_bytes(const vfrb_ddplan* plan, int64_t nt_out) {
   return plan ? vfrb::dedisperse_workspace_bytes_plan(plan, nt_out) : 0;
