@@ -192,6 +192,22 @@ typedef struct vfrb_dd_args {
 size_t vfrb_dedisperse_workspace_bytes(const vfrb_ddplan* plan, int64_t nt_out);
 int vfrb_dedisperse(const vfrb_ddplan* plan, const vfrb_dd_args* a, void* stream);
 
+/* vfrb_dedisperse without caller scratch (no counterpart in the reference,
+ * whose dedisperse + calcstats write into buffers it allocated at start-up).
+ * For callers that may not allocate device memory after start-up: the
+ * per-DM statistics partials go to a fixed device array of
+ * VFRB_NOALLOC_SCRATCH_BYTES per device instead of a->workspace, which is
+ * ignored; this call allocates nothing.  Requests whose
+ * vfrb_dedisperse_workspace_bytes exceed that size return VFRB_ERR_ARG and
+ * launch nothing.  The first call on each device looks up the array's
+ * address (make it before any stream capture).  All calls on one device
+ * share the array: calls whose work overlaps on the GPU (other streams,
+ * other threads) race and corrupt each other's statistics, so order them
+ * on one stream.  Nothing in the array needs to start at zero. */
+#define VFRB_NOALLOC_SCRATCH_BYTES (4u << 20)
+size_t vfrb_dedisperse_noalloc_scratch_bytes(void);
+int vfrb_dedisperse_noalloc(const vfrb_ddplan* plan, const vfrb_dd_args* a, void* stream);
+
 /* ---- K4: per-channel statistics (STATS:910-946) -------------------------
  * Per (channel, block of ncolstatblk rows): mean, variance ("sig") and the
  * outlier fraction count(x > ave + 5 sig)/npts with the reference's integer
