@@ -159,11 +159,15 @@ int vfrb_ddplan_group_size(const vfrb_ddplan* plan);
 #define VFRB_DD_REG2 3     /* register window, 2 adjacent trials per thread  */
 #define VFRB_DD_REG4 4     /* register window, 4 adjacent trials per thread  */
 #define VFRB_DD_DIRECT 5   /* direct loads (delay spreads too wide to stage) */
+#define VFRB_DD_PAT4 6     /* register window, 4 trials, runs of one delay pattern */
+#define VFRB_DD_PAT2 7     /* register window, 2 trials, runs of one delay pattern */
+#define VFRB_DD_NVARIANTS 8
 int vfrb_ddplan_set_variant(vfrb_ddplan* plan, int storage, int variant);
 int vfrb_ddplan_variant(const vfrb_ddplan* plan, int storage);
 /* Times every applicable variant on scratch data of the given shape
  * (nt_out samples per trial, `storage` form) and keeps the fastest.  Writes
- * the per-variant times in ms to times[6] (index = variant, < 0 = n/a). */
+ * the per-variant times in ms to times[VFRB_DD_NVARIANTS] (index = variant,
+ * < 0 = not applicable). */
 int vfrb_ddplan_autotune(vfrb_ddplan* plan, int storage, int64_t nt_out, float* times, void* stream);
 
 typedef struct vfrb_dd_args {
@@ -348,6 +352,45 @@ int vfrb_read_pairs(const uint8_t* bytes, size_t nbytes, int reader_mode, int da
 /* Reader log lines (frame skips, misalignment) of a stream, '\n'-joined;
  * valid until the next call.  Mirrors the reference's <OUT>.log messages. */
 const char* vfrb_stream_log(vfrb_plan* plan, int stream);
+
+/* MJD of the first frame pair a stream uses (getVDIFDMJD after initframe01,
+ * PIPE:525, STATS:365, TS:535): VFRB_OK once the reader has started,
+ * VFRB_PENDING before, VFRB_ERR when the stream failed to start. */
+int vfrb_stream_tstart(vfrb_plan* plan, int stream, double* mjd);
+
+/* ---- DADA-style input ring (host only) -----------------------------------
+ * The STATS and TS tools read VDIF from a psrdada ring (ipcio_connect /
+ * ipcio_open 'R' / ipcio_read / ipcbuf_eod: STATS:286-310, 444-462;
+ * TS:383-404, 767-826).  psrdada is not part of this build; this is a
+ * project-defined single-writer single-reader byte ring in POSIX shared
+ * memory named after the DADA key, with the same reader-side operations.
+ * All waits are bounded: reads and writes return -VFRB_ERR_TIMEOUT when
+ * nothing moved for timeout_ms. */
+typedef struct vfrb_dada vfrb_dada;
+/* capacity: data bytes, a power of two >= 4096.  Fails if the key exists. */
+int vfrb_dada_create(uint32_t key, uint64_t capacity, vfrb_dada** ring);
+int vfrb_dada_connect(uint32_t key, vfrb_dada** ring);
+/* Bytes written (all of them unless the wait ran out), or -status. */
+int64_t vfrb_dada_write(vfrb_dada* ring, const void* bytes, uint64_t n, int timeout_ms);
+int vfrb_dada_set_eod(vfrb_dada* ring);
+/* Bytes read: n, fewer at end of data (like ipcio_read), or -status. */
+int64_t vfrb_dada_read(vfrb_dada* ring, void* buf, uint64_t n, int timeout_ms);
+/* 1 when the writer has ended and every byte was read (ipcbuf_eod). */
+int vfrb_dada_eod(const vfrb_dada* ring);
+int vfrb_dada_close(vfrb_dada* ring);
+int vfrb_dada_destroy(uint32_t key);
+
+/* ---- output formats (host only) -----------------------------------------
+ * SIGPROC filterbank header as PIPE:529-540 writes it with the send_*
+ * helpers of PIPE:1177-1201 (keyword = int32 length + text, values native
+ * binary).  Returns the header length; writes it when cap is large enough. */
+size_t vfrb_sigproc_header(uint8_t* buf, size_t cap, double fch1, double foff, int32_t nchans, int32_t nbits,
+                           double tstart, double tsamp, int32_t nifs);
+/* PRESTO .inf text of the TS time series (writeprestoheader, TS:1483-1515).
+ * Returns the text length (excluding the NUL), writing it when cap > that;
+ * -1 on a NULL basename. */
+int vfrb_presto_inf(char* buf, size_t cap, const char* basename, double mjdstart, int32_t ntimes, double tsamp,
+                    float dm, double fchanlo, double bw, int32_t nchan, double chanbw);
 
 #ifdef __cplusplus
 }

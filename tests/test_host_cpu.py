@@ -2,6 +2,7 @@
 and its host-side arithmetic (header decode, MJD, layout, delay table)
 matches the oracle exactly."""
 import ctypes
+import ctypes as C
 import os
 import re
 
@@ -86,3 +87,31 @@ def test_dm1000_sweep(vf):
     L = vf.layout(12500, 10, 32, 384.0, 0, 60.0)
     off, md = vf.delay_table(L, np.array([1000.0], np.float32))
     assert 12600 < md < 12700 and off.max() <= md
+
+
+@pytest.mark.parametrize("fch1,foff,nch,tstart,tsamp", [(359.9949, -0.01024, 3908, 57083.6376284722, 0.000390625),
+                                                        (383.99488, -0.01024, 6250, 60311.25, 0.0009765625)])
+def test_sigproc_header_matches_oracle(vf, O, fch1, foff, nch, tstart, tsamp):
+    lib = vf.lib()
+    lib.vfrb_sigproc_header.restype = C.c_size_t
+    lib.vfrb_sigproc_header.argtypes = [C.c_void_p, C.c_size_t, C.c_double, C.c_double, C.c_int32, C.c_int32,
+                                        C.c_double, C.c_double, C.c_int32]
+    n = lib.vfrb_sigproc_header(None, 0, fch1, foff, nch, 32, tstart, tsamp, 1)
+    buf = (C.c_uint8 * n)()
+    assert lib.vfrb_sigproc_header(buf, n, fch1, foff, nch, 32, tstart, tsamp, 1) == n
+    assert bytes(buf) == O.sigproc_header(fch1, foff, nch, tstart, tsamp)
+
+
+def test_presto_inf_matches_oracle(vf, O):
+    lib = vf.lib()
+    lib.vfrb_presto_inf.restype = C.c_int
+    lib.vfrb_presto_inf.argtypes = [C.c_char_p, C.c_size_t, C.c_char_p, C.c_double, C.c_int32, C.c_double,
+                                    C.c_float, C.c_double, C.c_double, C.c_int32, C.c_double]
+    args = (b"DM119.3_2026-12-03_10:00:00", 60311.123456789012, 921600, 0.000390625, 119.3, 320.00512, 39.3216,
+            3840, 0.01024)
+    n = lib.vfrb_presto_inf(None, 0, *args)
+    buf = C.create_string_buffer(n + 1)
+    assert lib.vfrb_presto_inf(buf, n + 1, *args) == n
+    want = O.presto_inf(args[0].decode(), *args[1:])
+    assert buf.value.decode() == want
+    assert lib.vfrb_presto_inf(None, 0, None, *args[1:]) == -1

@@ -167,11 +167,13 @@ def test_bandpass_ring_in_and_out(vf, O):
     assert np.max(np.abs(got - ref)) <= 1e-6 * np.abs(x).max()
 
 
-def _dd_case(ndm=40, nch=256, nt=1000, seed=2, dm_max=30.0):
+def _dd_case(ndm=40, nch=256, nt=1000, seed=2, dm_max=30.0, irregular=False):
     rng = np.random.default_rng(seed)
     fch1, chanbw, tchan = 384.0, 0.25, 0.001
     from vfrb_oracle import delay_table
     dms = np.linspace(0, dm_max, ndm).astype(np.float32)
+    if irregular:  # unequal spacing: in-group delay patterns outside the straight-line table
+        dms = np.sort(rng.uniform(0, dm_max, ndm)).astype(np.float32)
     off, md = delay_table(dms, fch1, chanbw, tchan, nch)
     md = int(off.max())
     fb = rng.standard_normal((nt + md, nch)).astype(np.float32) * 3.0
@@ -208,14 +210,17 @@ def test_dedisperse_and_calcstats_match_fp64(vf, O):
     assert np.array_equal(st["argmax"].cpu().numpy(), st_ref["argmax"])
 
 
-@pytest.mark.parametrize("dm_max,ndm,group", [(8.0, 70, 4), (30.0, 40, 2), (120.0, 33, 1)])
+@pytest.mark.parametrize("dm_max,ndm,group,irregular",
+                         [(8.0, 70, 4, False), (30.0, 40, 2, False), (120.0, 33, 1, False), (8.0, 70, 4, True)])
 @pytest.mark.parametrize("storage,scaled", [(0, False), (1, False), (1, True)])
-def test_dedisperse_kernel_variants(vf, O, dm_max, ndm, group, storage, scaled):
+def test_dedisperse_kernel_variants(vf, O, dm_max, ndm, group, irregular, storage, scaled):
     """Every applicable kernel variant (register groups of 4/2/1 trials, the
-    staged and the direct kernel), FP32 and FP16 storage (one scale for all
-    channels, or per-channel weights), against the FP64 oracle."""
+    pattern-run kernels, the staged and the direct kernel), FP32 and FP16
+    storage (one scale for all channels, or per-channel weights), against the
+    FP64 oracle; the irregular DM list drives the pattern kernels' generic
+    path."""
     torch = _torch()
-    dms, off, md, fb = _dd_case(ndm=ndm, nch=320, nt=1500, seed=ndm, dm_max=dm_max)
+    dms, off, md, fb = _dd_case(ndm=ndm, nch=320, nt=1500, seed=ndm, dm_max=dm_max, irregular=irregular)
     nt = 1500
     plan = vf.DedispPlan(off)
     assert plan.group_size == group
@@ -235,6 +240,7 @@ def test_dedisperse_kernel_variants(vf, O, dm_max, ndm, group, storage, scaled):
     rms = np.sqrt(np.mean(ref ** 2))
     variants = [vf.DD_STAGED, vf.DD_DIRECT] + [{4: vf.DD_REG4, 2: vf.DD_REG2, 1: vf.DD_REG1}[g]
                                               for g in (4, 2, 1) if g <= group or g == group]
+    variants += [{4: vf.DD_PAT4, 2: vf.DD_PAT2}[g] for g in (4, 2) if g <= group]
     for v in sorted(set(variants)):
         plan.set_variant(storage, v)
         out, st = plan(x, nt, storage=storage, nrows_valid=rows, **kw)

@@ -164,3 +164,73 @@ def test_init_failure_matches_reference(tmp_path, vf, O):
     st_r, ref, _ = ref_bundles("pipe", str(p), 12500, 4, 32)
     st_p, prod, _ = product_bundles(vf, bad, 0, 12500, 4, 32)
     assert st_r == 2 and st_p == 2 and not ref and not prod
+
+
+def _libc():
+    libc = C.CDLL(None)
+    libc.fopen.restype = C.c_void_p
+    libc.fopen.argtypes = [C.c_char_p, C.c_char_p]
+    libc.fclose.argtypes = [C.c_void_p]
+    return libc
+
+
+def test_sigproc_header_matches_reference_helpers(vf, O, tmp_path):
+    """The reference's own send_string/send_int/send_double (PIPE:1177-1201)
+    called in the order of PIPE:529-540 give the oracle's and the product's
+    header bytes."""
+    lib = _reflib("pipe")
+    libc = _libc()
+    ss = getattr(lib, "_Z11send_stringPKcP8_IO_FILE")
+    si = getattr(lib, "_Z8send_intPKciP8_IO_FILE")
+    sd = getattr(lib, "_Z11send_doublePKcdP8_IO_FILE")
+    ss.argtypes = [C.c_char_p, C.c_void_p]
+    si.argtypes = [C.c_char_p, C.c_int, C.c_void_p]
+    sd.argtypes = [C.c_char_p, C.c_double, C.c_void_p]
+    fch1, foff, nch, tstart, tsamp = 359.9949, -0.01024, 3908, 57083.6376284722, 0.000390625
+    path = str(tmp_path / "x.head").encode()
+    f = libc.fopen(path, b"wb")
+    assert f
+    ss(b"HEADER_START", f)
+    si(b"barycentric", 1, f)
+    si(b"telescope_id", 12, f)
+    si(b"data_type", 1, f)
+    sd(b"fch1", fch1, f)
+    sd(b"foff", foff, f)
+    si(b"nchans", nch, f)
+    si(b"nbits", 32, f)
+    sd(b"tstart", tstart, f)
+    sd(b"tsamp", tsamp, f)
+    si(b"nifs", 1, f)
+    ss(b"HEADER_END", f)
+    libc.fclose(f)
+    ref = open(path, "rb").read()
+    assert ref == O.sigproc_header(fch1, foff, nch, tstart, tsamp)
+    plib = vf.lib()
+    plib.vfrb_sigproc_header.restype = C.c_size_t
+    plib.vfrb_sigproc_header.argtypes = [C.c_void_p, C.c_size_t, C.c_double, C.c_double, C.c_int32, C.c_int32,
+                                         C.c_double, C.c_double, C.c_int32]
+    buf = (C.c_uint8 * len(ref))()
+    assert plib.vfrb_sigproc_header(buf, len(ref), fch1, foff, nch, 32, tstart, tsamp, 1) == len(ref)
+    assert bytes(buf) == ref
+
+
+def test_presto_inf_matches_reference(vf, O, tmp_path):
+    """writeprestoheader (TS:1483-1515) itself, against the oracle and the
+    product."""
+    lib = _reflib("ts")
+    wp = getattr(lib, "_Z17writeprestoheaderPcdidfddid")
+    wp.argtypes = [C.c_char_p, C.c_double, C.c_int, C.c_double, C.c_float, C.c_double, C.c_double, C.c_int,
+                   C.c_double]
+    wp.restype = C.c_int
+    base = str(tmp_path / "DM119.3_2026-12-03_10:00:00")
+    args = (60311.123456789012, 921600, 0.000390625, 119.3, 320.00512, 39.3216, 3840, 0.01024)
+    assert wp(base.encode(), *args) == 0
+    ref = open(base + ".inf").read()
+    assert ref == O.presto_inf(base, *args)
+    plib = vf.lib()
+    plib.vfrb_presto_inf.restype = C.c_int
+    plib.vfrb_presto_inf.argtypes = [C.c_char_p, C.c_size_t, C.c_char_p, C.c_double, C.c_int32, C.c_double,
+                                     C.c_float, C.c_double, C.c_double, C.c_int32, C.c_double]
+    buf = C.create_string_buffer(4096)
+    assert plib.vfrb_presto_inf(buf, 4096, base.encode(), *args) == len(ref)
+    assert buf.value.decode() == ref

@@ -18,7 +18,8 @@ LIB_PATH = os.path.join(_HERE, "lib", "libvfrb.so")
 
 VFRB_OK, VFRB_EOD, VFRB_ERR = 0, 1, 2
 F32, F16, I8 = 0, 1, 2
-DD_AUTO, DD_STAGED, DD_REG1, DD_REG2, DD_REG4, DD_DIRECT = 0, 1, 2, 3, 4, 5
+DD_AUTO, DD_STAGED, DD_REG1, DD_REG2, DD_REG4, DD_DIRECT, DD_PAT4, DD_PAT2 = 0, 1, 2, 3, 4, 5, 6, 7
+DD_NVARIANTS = 8
 
 
 class VfrbError(RuntimeError):
@@ -223,9 +224,9 @@ class DedispPlan:
 
     def autotune(self, storage: int, nt_out: int, stream=None):
         """Times each applicable kernel variant; returns {variant: ms} (n/a omitted)."""
-        t = (C.c_float * 6)()
+        t = (C.c_float * DD_NVARIANTS)()
         _check(_lib.vfrb_ddplan_autotune(self._p, storage, nt_out, t, _stream(stream)), "vfrb_ddplan_autotune")
-        return {i: t[i] for i in range(1, 6) if t[i] >= 0}
+        return {i: t[i] for i in range(1, DD_NVARIANTS) if t[i] >= 0}
 
     def workspace_bytes(self, nt_out: int) -> int:
         return int(_lib.vfrb_dedisperse_workspace_bytes(self._p, nt_out))

@@ -53,6 +53,9 @@ def gen_codelets():
         txt = subprocess.run([sys.executable, gen], capture_output=True, text=True, check=True).stdout
         with open(out, "w") as f:
             f.write(txt)
+    pat = os.path.join(CSRC, "gen_patterns.py")
+    if _newer(pat, os.path.join(CSRC, "dedisp_patterns.cuh")):
+        subprocess.run([sys.executable, pat], check=True)
 
 
 def build(jobs: int = 8, verbose: bool = False) -> str:

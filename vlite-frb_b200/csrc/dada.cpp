@@ -1,0 +1,202 @@
+// Shared-memory byte ring for the DADA-fed tools (host only).
+//
+// The reference's STATS and TS tools read their VDIF stream from a psrdada
+// ring with ipcio_connect / ipcio_open('R') / ipcio_read / ipcbuf_eod
+// (STATS:286-310, 444-462; TS:383-404, 767-826).  psrdada is not part of this
+// build, so this is a project-defined ring with the same reader-side
+// operations: one writer and one reader process share a POSIX shared-memory
+// object named after the DADA key; the writer appends bytes and finally marks
+// end of data; the reader gets the bytes in order, and a short read means end
+// of data.  Every wait is bounded (timeout_ms) and reports VFRB_ERR_TIMEOUT.
+#include <fcntl.h>
+#include <sys/mman.h>
+#include <sys/stat.h>
+#include <time.h>
+#include <unistd.h>
+
+#include <atomic>
+#include <new>
+#include <cstdint>
+#include <cstdio>
+#include <cstring>
+
+#include "vfrb.h"
+
+namespace {
+
+constexpr uint64_t kMagic = 0x7666726264616461ULL;  // "vfrbdada"
+
+struct RingHdr {
+  uint64_t magic;
+  uint64_t cap;                    // data bytes (power of two)
+  std::atomic<uint64_t> wpos;      // bytes written so far
+  std::atomic<uint64_t> rpos;      // bytes consumed so far
+  std::atomic<uint32_t> eod;       // writer finished
+  uint32_t pad;
+};
+static_assert(sizeof(RingHdr) <= 64, "header fits one cache line");
+constexpr size_t kHdrBytes = 64;
+
+void shm_name(uint32_t key, char* out, size_t n) { std::snprintf(out, n, "/vfrb_dada_%08x", key); }
+
+void nap() {
+  timespec ts{0, 100000};  // 0.1 ms
+  nanosleep(&ts, nullptr);
+}
+
+double now_ms() {
+  timespec ts;
+  clock_gettime(CLOCK_MONOTONIC, &ts);
+  return ts.tv_sec * 1e3 + ts.tv_nsec * 1e-6;
+}
+
+}  // namespace
+
+struct vfrb_dada {
+  uint32_t key = 0;
+  RingHdr* h = nullptr;
+  uint8_t* data = nullptr;
+  size_t map_bytes = 0;
+};
+
+extern "C" {
+
+int vfrb_dada_create(uint32_t key, uint64_t capacity, vfrb_dada** out) {
+  if (!out || capacity < 4096 || (capacity & (capacity - 1))) return VFRB_ERR_ARG;
+  char name[64];
+  shm_name(key, name, sizeof name);
+  const int fd = shm_open(name, O_CREAT | O_EXCL | O_RDWR, 0600);
+  if (fd < 0) return VFRB_ERR;
+  const size_t bytes = kHdrBytes + capacity;
+  if (ftruncate(fd, (off_t)bytes) != 0) {
+    close(fd);
+    shm_unlink(name);
+    return VFRB_ERR_NOMEM;
+  }
+  void* p = mmap(nullptr, bytes, PROT_READ | PROT_WRITE, MAP_SHARED, fd, 0);
+  close(fd);
+  if (p == MAP_FAILED) {
+    shm_unlink(name);
+    return VFRB_ERR_NOMEM;
+  }
+  auto* d = new vfrb_dada();
+  d->key = key;
+  d->h = new (p) RingHdr();
+  d->h->cap = capacity;
+  d->h->wpos.store(0);
+  d->h->rpos.store(0);
+  d->h->eod.store(0);
+  d->data = static_cast<uint8_t*>(p) + kHdrBytes;
+  d->map_bytes = bytes;
+  std::atomic_thread_fence(std::memory_order_release);
+  d->h->magic = kMagic;
+  *out = d;
+  return VFRB_OK;
+}
+
+int vfrb_dada_connect(uint32_t key, vfrb_dada** out) {
+  if (!out) return VFRB_ERR_ARG;
+  char name[64];
+  shm_name(key, name, sizeof name);
+  const int fd = shm_open(name, O_RDWR, 0600);
+  if (fd < 0) return VFRB_ERR;
+  struct stat sb;
+  if (fstat(fd, &sb) != 0 || (size_t)sb.st_size < kHdrBytes + 4096) {
+    close(fd);
+    return VFRB_ERR;
+  }
+  void* p = mmap(nullptr, (size_t)sb.st_size, PROT_READ | PROT_WRITE, MAP_SHARED, fd, 0);
+  close(fd);
+  if (p == MAP_FAILED) return VFRB_ERR_NOMEM;
+  auto* h = static_cast<RingHdr*>(p);
+  if (h->magic != kMagic || kHdrBytes + h->cap != (size_t)sb.st_size) {
+    munmap(p, (size_t)sb.st_size);
+    return VFRB_ERR;
+  }
+  auto* d = new vfrb_dada();
+  d->key = key;
+  d->h = h;
+  d->data = static_cast<uint8_t*>(p) + kHdrBytes;
+  d->map_bytes = (size_t)sb.st_size;
+  *out = d;
+  return VFRB_OK;
+}
+
+int64_t vfrb_dada_write(vfrb_dada* d, const void* bytes, uint64_t n, int timeout_ms) {
+  if (!d || (!bytes && n)) return -VFRB_ERR_ARG;
+  const uint64_t cap = d->h->cap;
+  const auto* src = static_cast<const uint8_t*>(bytes);
+  uint64_t done = 0;
+  double t0 = now_ms();
+  while (done < n) {
+    const uint64_t w = d->h->wpos.load(std::memory_order_relaxed);
+    const uint64_t r = d->h->rpos.load(std::memory_order_acquire);
+    const uint64_t room = cap - (w - r);
+    if (room == 0) {
+      if (now_ms() - t0 > timeout_ms) return done ? (int64_t)done : -VFRB_ERR_TIMEOUT;
+      nap();
+      continue;
+    }
+    uint64_t k = n - done < room ? n - done : room;
+    const uint64_t at = w & (cap - 1);
+    if (k > cap - at) k = cap - at;
+    std::memcpy(d->data + at, src + done, k);
+    d->h->wpos.store(w + k, std::memory_order_release);
+    done += k;
+    t0 = now_ms();
+  }
+  return (int64_t)done;
+}
+
+int vfrb_dada_set_eod(vfrb_dada* d) {
+  if (!d) return VFRB_ERR_ARG;
+  d->h->eod.store(1, std::memory_order_release);
+  return VFRB_OK;
+}
+
+int64_t vfrb_dada_read(vfrb_dada* d, void* buf, uint64_t n, int timeout_ms) {
+  if (!d || (!buf && n)) return -VFRB_ERR_ARG;
+  const uint64_t cap = d->h->cap;
+  auto* dst = static_cast<uint8_t*>(buf);
+  uint64_t done = 0;
+  double t0 = now_ms();
+  while (done < n) {
+    const uint64_t r = d->h->rpos.load(std::memory_order_relaxed);
+    const uint64_t w = d->h->wpos.load(std::memory_order_acquire);
+    if (w == r) {
+      if (d->h->eod.load(std::memory_order_acquire) && d->h->wpos.load(std::memory_order_acquire) == r) break;
+      if (now_ms() - t0 > timeout_ms) return done ? (int64_t)done : -VFRB_ERR_TIMEOUT;
+      nap();
+      continue;
+    }
+    uint64_t k = w - r < n - done ? w - r : n - done;
+    const uint64_t at = r & (cap - 1);
+    if (k > cap - at) k = cap - at;
+    std::memcpy(dst + done, d->data + at, k);
+    d->h->rpos.store(r + k, std::memory_order_release);
+    done += k;
+    t0 = now_ms();
+  }
+  return (int64_t)done;
+}
+
+int vfrb_dada_eod(const vfrb_dada* d) {
+  if (!d) return VFRB_ERR_ARG;
+  return d->h->eod.load(std::memory_order_acquire) &&
+         d->h->wpos.load(std::memory_order_acquire) == d->h->rpos.load(std::memory_order_acquire);
+}
+
+int vfrb_dada_close(vfrb_dada* d) {
+  if (!d) return VFRB_ERR_ARG;
+  munmap(d->h, d->map_bytes);
+  delete d;
+  return VFRB_OK;
+}
+
+int vfrb_dada_destroy(uint32_t key) {
+  char name[64];
+  shm_name(key, name, sizeof name);
+  return shm_unlink(name) == 0 ? VFRB_OK : VFRB_ERR;
+}
+
+}  // extern "C"

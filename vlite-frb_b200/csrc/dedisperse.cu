@@ -349,6 +349,7 @@ __global__ void __launch_bounds__(256) k_dedisperse_direct(const DdKParams p) {
 }  // namespace vfrb
 
 #include "dedisperse_reg.cuh"
+#include "dedisperse_pat.cuh"
 
 
 // ---- plan object --------------------------------------------------------------
@@ -364,6 +365,8 @@ struct RegGroup {
   int* d_gbase = nullptr;
   unsigned* d_gpack = nullptr;
   int* d_bmin = nullptr;
+  unsigned char* d_gpat = nullptr;  // pattern id per (group, channel), D = 4 and 2
+  long long n_generic = 0;          // (group, channel) pairs outside the pattern table
 };
 }  // namespace vfrb
 
@@ -491,7 +494,80 @@ static int reg_launch(const vfrb_ddplan* pl, int v, const vfrb_dd_args& a, DmPar
   return VFRB_OK;
 }
 
+template <typename T, int D, int TT, int SMAX>
+static int pat_launch_t(const vfrb_ddplan* pl, const RegGroup& g, const vfrb_dd_args& a, DmPartial* part,
+                        float out_scale, cudaStream_t s, int* ntb) {
+  constexpr int VEC = 16 / (int)sizeof(T);
+  constexpr int NT = 32 * TT;
+  *ntb = 0;
+  if (g.D != D || g.smax > SMAX || !g.d_gpat) return VFRB_OK;  // not applicable
+  const int lm = (g.span + VEC - 1 + NT + SMAX + VEC - 1) / VEC * VEC;
+  // two CTAs per SM: keep each under ~110 KB of shared memory
+  const int per_ch = 2 * lm * (int)sizeof(T) + 3 * 2 * kPatWarps * 4;
+  const int chunk = std::min(32, (110 * 1024 - 2 * kPatWarps * 4 - 16) / per_ch);
+  if (chunk < 4) return VFRB_OK;
+  DdPatParams k{};
+  k.fb = a.fb;
+  k.out_scale = out_scale;
+  k.chan_stride = a.chan_stride;
+  k.row0 = a.row0;
+  k.row_mask = a.row_mask;
+  k.nrows_valid = a.nrows_valid;
+  k.nchan = pl->nchan;
+  k.ndm = pl->ndm;
+  k.ngroups = g.ngroups;
+  k.nt_out = a.nt_out;
+  k.out = a.out;
+  k.out_stride = a.out_stride;
+  k.part = part;
+  k.gbase = g.d_gbase;
+  k.gpack = g.d_gpack;
+  k.gpat = g.d_gpat;
+  k.bmin = g.d_bmin;
+  k.chunk = chunk;
+  k.lmax = lm;
+  k.err = a.d_err;
+  const size_t meta = ((size_t)3 * 2 * kPatWarps * chunk + 2 * kPatWarps + 3) / 4 * 16;
+  const size_t smem = meta + (size_t)2 * chunk * lm * sizeof(T);
+  cudaError_t e =
+      cudaFuncSetAttribute(k_dedisp_pat<T, D, TT, SMAX>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return VFRB_ERR_CUDA;
+  dim3 grid((unsigned)((a.nt_out + NT - 1) / NT), (unsigned)g.nblocks);
+  k_dedisp_pat<T, D, TT, SMAX><<<grid, kPatWarps * 32, smem, s>>>(k);
+  const int st = cuda_status(cudaGetLastError());
+  if (st == VFRB_OK) *ntb = (int)grid.x;
+  return st;
+}
+
+// Pattern-run variant `v` for this call; *ntb == 0 when it does not apply.
+static int pat_launch(const vfrb_ddplan* pl, int v, const vfrb_dd_args& a, DmPartial* part, cudaStream_t s,
+                      int* ntb) {
+  *ntb = 0;
+  if (((uintptr_t)a.fb & 15) != 0) return VFRB_OK;
+  const int D = v == VFRB_DD_PAT4 ? 4 : 2;
+  const RegGroup* g = find_group(pl, D);
+  if (!g) return VFRB_OK;
+  if (a.storage == VFRB_F32) {
+    if (a.chan_stride % 4 || ((unsigned long long)a.row_mask + 1ULL) % 4) return VFRB_OK;
+    if (D == 4) return pat_launch_t<float, 4, 15, VFRB_PAT4_SMAX>(pl, *g, a, part, 1.f, s, ntb);
+    return pat_launch_t<float, 2, 27, VFRB_PAT2_SMAX>(pl, *g, a, part, 1.f, s, ntb);
+  }
+  if (a.storage == VFRB_F16) {
+    if (a.chan_scale || !(a.uniform_scale > 0.f)) return VFRB_OK;
+    if (a.chan_stride % 8 || ((unsigned long long)a.row_mask + 1ULL) % 8) return VFRB_OK;
+    if (D == 4) return pat_launch_t<__half, 4, 14, VFRB_PAT4_SMAX>(pl, *g, a, part, a.uniform_scale, s, ntb);
+    return pat_launch_t<__half, 2, 26, VFRB_PAT2_SMAX>(pl, *g, a, part, a.uniform_scale, s, ntb);
+  }
+  return VFRB_OK;
+}
+
 static int default_variant(const vfrb_ddplan* pl, int storage) {
+  if (storage == VFRB_F32 || storage == VFRB_F16) {
+    const RegGroup* g4 = find_group(pl, 4);
+    const RegGroup* g2 = find_group(pl, 2);
+    if (g4 && g4->d_gpat) return VFRB_DD_PAT4;
+    if (g2 && g2->d_gpat) return VFRB_DD_PAT2;
+  }
   if (storage == VFRB_F32) {
     if (find_group(pl, 4)) return VFRB_DD_REG4;
     if (find_group(pl, 2)) return VFRB_DD_REG2;
@@ -526,6 +602,7 @@ static int launch_variant(const vfrb_ddplan* pl, int v, const vfrb_dd_args& a, c
   int ntb = 0, st = VFRB_OK;
   if (!a.sigma_out && (v == VFRB_DD_REG1 || v == VFRB_DD_REG2 || v == VFRB_DD_REG4))
     st = reg_launch(pl, v, a, k.part, s, &ntb);
+  if (!a.sigma_out && (v == VFRB_DD_PAT4 || v == VFRB_DD_PAT2)) st = pat_launch(pl, v, a, k.part, s, &ntb);
   if (st) return st;
   if (ntb == 0) {
     const bool staged = v != VFRB_DD_DIRECT;
@@ -619,13 +696,19 @@ int ddplan_autotune(vfrb_ddplan* pl, int storage, long long nt, float* times, cu
   cudaEventCreate(&e1);
   float best = 1e30f;
   int bestv = VFRB_DD_STAGED;
-  for (int v = VFRB_DD_STAGED; v <= VFRB_DD_DIRECT; ++v) {
+  if (times) times[VFRB_DD_AUTO] = -1.f;
+  // the direct variant last: it is timed only when nothing faster applies
+  static const int order[] = {VFRB_DD_STAGED, VFRB_DD_REG1, VFRB_DD_REG2, VFRB_DD_REG4,
+                              VFRB_DD_PAT2,   VFRB_DD_PAT4, VFRB_DD_DIRECT};
+  for (int v : order) {
     if (times) times[v] = -1.f;
-    if (v == VFRB_DD_DIRECT && bestv != VFRB_DD_STAGED) continue;  // only when nothing faster applies
+    if (v == VFRB_DD_DIRECT && bestv != VFRB_DD_STAGED) continue;
     const bool reg = v == VFRB_DD_REG1 || v == VFRB_DD_REG2 || v == VFRB_DD_REG4;
-    if (reg) {
-      const int D = v == VFRB_DD_REG4 ? 4 : v == VFRB_DD_REG2 ? 2 : 1;
-      if (!find_group(pl, D) || storage == VFRB_I8) continue;
+    const bool pat = v == VFRB_DD_PAT2 || v == VFRB_DD_PAT4;
+    if (reg || pat) {
+      const int D = v == VFRB_DD_REG4 || v == VFRB_DD_PAT4 ? 4 : v == VFRB_DD_REG2 || v == VFRB_DD_PAT2 ? 2 : 1;
+      const RegGroup* g = find_group(pl, D);
+      if (!g || storage == VFRB_I8 || (pat && !g->d_gpat)) continue;
     }
     if (launch_variant(pl, v, a, s) != VFRB_OK) continue;  // warm-up; also rejects what does not apply
     cudaEventRecord(e0, s);
@@ -651,7 +734,8 @@ int ddplan_autotune(vfrb_ddplan* pl, int storage, long long nt, float* times, cu
 }
 
 int ddplan_set_variant(vfrb_ddplan* pl, int storage, int v) {
-  if (!pl || storage < VFRB_F32 || storage > VFRB_I8 || v < VFRB_DD_AUTO || v > VFRB_DD_DIRECT) return VFRB_ERR_ARG;
+  if (!pl || storage < VFRB_F32 || storage > VFRB_I8 || v < VFRB_DD_AUTO || v >= VFRB_DD_NVARIANTS)
+    return VFRB_ERR_ARG;
   pl->variant[storage] = v;
   return VFRB_OK;
 }
@@ -659,6 +743,33 @@ int ddplan_set_variant(vfrb_ddplan* pl, int storage, int v) {
 int ddplan_variant(const vfrb_ddplan* pl, int storage) {
   if (!pl || storage < VFRB_F32 || storage > VFRB_I8) return -1;
   return pl->variant[storage] == VFRB_DD_AUTO ? default_variant(pl, storage) : pl->variant[storage];
+}
+
+// Pattern id of the packed in-group differences (8 bits per trial, trial 0
+// first), kPatGeneric when the pattern has no straight-line code.
+static unsigned char pattern_id(int D, unsigned pk) {
+  static const std::vector<unsigned char> lut4 = [] {
+    std::vector<unsigned char> t(1u << 15, kPatGeneric);
+#define VFRB_L4(ID, A, B, C) t[(unsigned)(A) | ((unsigned)(B) << 5) | ((unsigned)(C) << 10)] = (unsigned char)(ID);
+    VFRB_PAT4_LIST(VFRB_L4)
+#undef VFRB_L4
+    return t;
+  }();
+  static const std::vector<unsigned char> lut2 = [] {
+    std::vector<unsigned char> t(256, kPatGeneric);
+#define VFRB_L2(ID, A) t[(unsigned)(A)] = (unsigned char)(ID);
+    VFRB_PAT2_LIST(VFRB_L2)
+#undef VFRB_L2
+    return t;
+  }();
+  if ((pk & 0xFFu) != 0) return kPatGeneric;  // trial 0 must have the smallest delay
+  if (D == 4) {
+    const unsigned a = (pk >> 8) & 0xFFu, b = (pk >> 16) & 0xFFu, c = pk >> 24;
+    if (a > 31 || b > 31 || c > 31) return kPatGeneric;
+    return lut4[a | (b << 5) | (c << 10)];
+  }
+  if (D == 2) return lut2[(pk >> 8) & 0xFFu];
+  return kPatGeneric;
 }
 
 static int build_group(vfrb_ddplan* p, const int32_t* h_off, int D, int smax_allowed) {
@@ -707,17 +818,29 @@ static int build_group(vfrb_ddplan* p, const int32_t* h_off, int D, int smax_all
   g.span = span;
   g.ngroups = ng;
   g.nblocks = nb;
+  const bool with_pat = (D == 4 && smax <= VFRB_PAT4_SMAX) || (D == 2 && smax <= VFRB_PAT2_SMAX);
+  std::vector<unsigned char> pt;
+  if (with_pat) {
+    pt.resize(gp.size());
+    for (size_t i = 0; i < gp.size(); ++i) {
+      pt[i] = pattern_id(D, gp[i]);
+      g.n_generic += pt[i] == kPatGeneric;
+    }
+  }
   bool ok = cudaMalloc(&g.d_gbase, gb.size() * sizeof(int)) == cudaSuccess &&
             cudaMalloc(&g.d_gpack, gp.size() * sizeof(unsigned)) == cudaSuccess &&
-            cudaMalloc(&g.d_bmin, bm.size() * sizeof(int)) == cudaSuccess;
+            cudaMalloc(&g.d_bmin, bm.size() * sizeof(int)) == cudaSuccess &&
+            (!with_pat || cudaMalloc(&g.d_gpat, pt.size()) == cudaSuccess);
   ok = ok && cudaMemcpy(g.d_gbase, gb.data(), gb.size() * sizeof(int), cudaMemcpyHostToDevice) == cudaSuccess &&
        cudaMemcpy(g.d_gpack, gp.data(), gp.size() * sizeof(unsigned), cudaMemcpyHostToDevice) == cudaSuccess &&
-       cudaMemcpy(g.d_bmin, bm.data(), bm.size() * sizeof(int), cudaMemcpyHostToDevice) == cudaSuccess;
+       cudaMemcpy(g.d_bmin, bm.data(), bm.size() * sizeof(int), cudaMemcpyHostToDevice) == cudaSuccess &&
+       (!with_pat || cudaMemcpy(g.d_gpat, pt.data(), pt.size(), cudaMemcpyHostToDevice) == cudaSuccess);
   if (!ok) {
     cudaGetLastError();
     cudaFree(g.d_gbase);
     cudaFree(g.d_gpack);
     cudaFree(g.d_bmin);
+    cudaFree(g.d_gpat);
     return VFRB_ERR_NOMEM;
   }
   *slot = g;
@@ -731,6 +854,7 @@ int ddplan_destroy(vfrb_ddplan* p) {
     if (g.d_gbase) cudaFree(g.d_gbase);
     if (g.d_gpack) cudaFree(g.d_gpack);
     if (g.d_bmin) cudaFree(g.d_bmin);
+    if (g.d_gpat) cudaFree(g.d_gpat);
   }
   delete p;
   return VFRB_OK;
@@ -782,7 +906,7 @@ int ddplan_create(vfrb_ddplan** out, const int32_t* h_off, int ndm, int nchan) {
 int ddplan_max_delay(const vfrb_ddplan* p) { return p->max_delay; }
 int ddplan_reg_group(const vfrb_ddplan* p) {
   const int v = ddplan_variant(p, VFRB_F32);
-  return v == VFRB_DD_REG4 ? 4 : v == VFRB_DD_REG2 ? 2 : v == VFRB_DD_REG1 ? 1 : 0;
+  return v == VFRB_DD_REG4 || v == VFRB_DD_PAT4 ? 4 : v == VFRB_DD_REG2 || v == VFRB_DD_PAT2 ? 2 : v == VFRB_DD_REG1 ? 1 : 0;
 }
 
 }  // namespace vfrb

@@ -1,0 +1,321 @@
+// Pattern-run dedispersion kernel (included by dedisperse.cu, after
+// dedisperse_reg.cuh).
+//
+// Like the register-window kernel, each thread owns D adjacent DM trials (a
+// "group") x TT consecutive output samples and, per channel, loads ONE window
+// of TT + Delta_max samples from the shared-memory tile into registers and
+// adds it at each trial's delay difference Delta_j, so one shared load feeds
+// up to D additions.  The difference is how the shifts reach the code:
+//
+//  * windows are read with 4-byte (FP32) or 2-byte (FP16) loads at any
+//    element offset, so there is no 16-byte alignment residual and the shift
+//    of trial j is exactly Delta_j(group, channel);
+//  * for equally spaced DM trials Delta_j = floor(phi + j*y) takes only a
+//    few dozen distinct patterns (dedisp_patterns.cuh), so the kernel has
+//    straight-line code per pattern;
+//  * when a chunk of channels is staged, each warp sorts its channels by
+//    pattern (warp match + prefix sum) into runs, and the summation loop
+//    dispatches once per run instead of once per (trial, channel).
+//
+// Lanes own TT-sample runs with TT odd (FP32) or TT = 2 mod 4 (FP16), so the
+// 32 lanes of a load touch 32 different banks.  Groups whose pattern is not
+// in the table take a generic path (one dispatch per trial and channel).
+#pragma once
+
+#include "dedisp_patterns.cuh"
+
+namespace vfrb {
+
+constexpr int kPatWarps = 8;
+constexpr unsigned char kPatGeneric = 255;
+
+struct DdPatParams {
+  const void* fb;
+  float out_scale;  // multiplies sum/nchan (1 for FP32, S for FP16)
+  long long chan_stride;
+  long long row0;
+  unsigned row_mask;
+  long long nrows_valid;
+  int nchan;
+  int ndm;
+  int ngroups;
+  long long nt_out;
+  float* out;
+  long long out_stride;
+  DmPartial* part;
+  const int* gbase;            // [ngroups][nchan] smallest delay of the group
+  const unsigned* gpack;       // [ngroups][nchan] D delay differences, 8 bits each
+  const unsigned char* gpat;   // [ngroups][nchan] pattern id, kPatGeneric if none
+  const int* bmin;             // [nblocks][nchan] smallest delay of a CTA's trials
+  int chunk;                   // channels per stage (<= 32)
+  int lmax;                    // tile row length in elements (multiple of 16 bytes)
+  int* err;
+};
+
+template <typename T>
+struct PatElem;
+template <>
+struct PatElem<float> {
+  using R = float;
+  __device__ __forceinline__ static R load(const float* p) { return *p; }
+  __device__ __forceinline__ static float add(float a, R v) { return a + v; }
+};
+template <>
+struct PatElem<__half> {
+  using R = unsigned short;
+  __device__ __forceinline__ static R load(const __half* p) { return *reinterpret_cast<const unsigned short*>(p); }
+  __device__ __forceinline__ static float add(float a, R v) { return add_h(a, v); }
+};
+
+template <int A, int... R>
+struct PatMax {
+  static constexpr int v = A > PatMax<R...>::v ? A : PatMax<R...>::v;
+};
+template <int A>
+struct PatMax<A> {
+  static constexpr int v = A;
+};
+
+// acc[J + i][t] += w[t + S_i] for the trials J, J+1, ... with shifts S...
+template <typename T, int D, int TT, int NW, int J, int S0, int... SR>
+__device__ __forceinline__ void pat_add(float (&acc)[D][TT], const typename PatElem<T>::R (&w)[NW]) {
+#pragma unroll
+  for (int t = 0; t < TT; ++t) acc[J][t] = PatElem<T>::add(acc[J][t], w[t + S0]);
+  if constexpr (sizeof...(SR) > 0) pat_add<T, D, TT, NW, J + 1, SR...>(acc, w);
+}
+
+// n channels of one run: window loads + static-shift adds
+template <typename T, int D, int TT, int... S>
+__device__ __forceinline__ void pat_run(float (&acc)[D][TT], const T* tile, const int* slot, int n, int lane_off) {
+  constexpr int NW = TT + PatMax<S...>::v;
+  using R = typename PatElem<T>::R;
+#pragma unroll 1
+  for (int i = 0; i < n; ++i) {
+    const T* src = tile + slot[i] + lane_off;
+    R w[NW];
+#pragma unroll
+    for (int k = 0; k < NW; ++k) w[k] = PatElem<T>::load(src + k);
+    pat_add<T, D, TT, NW, 0, S...>(acc, w);
+  }
+}
+
+template <typename T, int TT, int NW, int S>
+__device__ __forceinline__ void pat_add_one(float (&acc)[TT], const typename PatElem<T>::R (&w)[NW]) {
+#pragma unroll
+  for (int t = 0; t < TT; ++t) acc[t] = PatElem<T>::add(acc[t], w[t + S]);
+}
+
+// generic path: per channel, one dispatch per trial on its shift
+template <typename T, int D, int TT, int SMAX>
+__device__ __forceinline__ void pat_run_generic(float (&acc)[D][TT], const T* tile, const int* slot, const unsigned* pk,
+                                             int n, int lane_off) {
+  constexpr int NW = TT + SMAX;
+  using R = typename PatElem<T>::R;
+#pragma unroll 1
+  for (int i = 0; i < n; ++i) {
+    const T* src = tile + slot[i] + lane_off;
+    R w[NW];
+#pragma unroll
+    for (int k = 0; k < NW; ++k) w[k] = PatElem<T>::load(src + k);
+    const unsigned sh = pk[i];
+#pragma unroll
+    for (int j = 0; j < D; ++j) {
+      switch ((int)((sh >> (8 * j)) & 0xFFu)) {
+#define VFRB_G(S)                                                       \
+  case S:                                                               \
+    if constexpr (S <= SMAX) pat_add_one<T, TT, NW, S>(acc[j], w);      \
+    break;
+        VFRB_CASES_0_31(VFRB_G)
+#undef VFRB_G
+        default:
+          break;
+      }
+    }
+  }
+}
+
+template <typename T, int D, int TT, int SMAX>
+__device__ __forceinline__ void pat_dispatch(float (&acc)[D][TT], int pat, const T* tile, const int* slot,
+                                             const unsigned* pk, int n, int lane_off) {
+  if constexpr (D == 4) {
+    switch (pat) {
+#define VFRB_P4(ID, A, B, C)                                                           \
+  case ID:                                                                             \
+    if constexpr (PatMax<A, B, C>::v <= SMAX) pat_run<T, D, TT, 0, A, B, C>(acc, tile, slot, n, lane_off); \
+    return;
+      VFRB_PAT4_LIST(VFRB_P4)
+#undef VFRB_P4
+      default:
+        break;
+    }
+  } else if constexpr (D == 2) {
+    switch (pat) {
+#define VFRB_P2(ID, A)                                                               \
+  case ID:                                                                           \
+    if constexpr (A <= SMAX) pat_run<T, D, TT, 0, A>(acc, tile, slot, n, lane_off);  \
+    return;
+      VFRB_PAT2_LIST(VFRB_P2)
+#undef VFRB_P2
+      default:
+        break;
+    }
+  }
+  pat_run_generic<T, D, TT, SMAX>(acc, tile, slot, pk, n, lane_off);
+}
+
+template <typename T, int D, int TT, int SMAX>
+__global__ void __launch_bounds__(kPatWarps * 32, 2) k_dedisp_pat(const DdPatParams p) {
+  constexpr int VEC = 16 / (int)sizeof(T);
+  constexpr int NT = 32 * TT;
+  static_assert(sizeof(T) == 4 ? (TT & 1) == 1 : (TT & 3) == 2, "lane stride must spread loads over all banks");
+  extern __shared__ int4 smp4[];
+  const int CH = p.chunk, LM = p.lmax;
+  const int LMQ = LM / VEC;
+  // shared layout: slot[2][W][CH] int, pk[2][W][CH] unsigned, run[2][W][CH] int, nrun[2][W] int, tiles[2][CH][LM]
+  int* s_slot = reinterpret_cast<int*>(smp4);
+  unsigned* s_pk = reinterpret_cast<unsigned*>(s_slot + 2 * kPatWarps * CH);
+  int* s_run = reinterpret_cast<int*>(s_pk + 2 * kPatWarps * CH);
+  int* s_nrun = s_run + 2 * kPatWarps * CH;
+  const int meta_q = (3 * 2 * kPatWarps * CH + 2 * kPatWarps + 3) / 4;
+  int4* tiles = smp4 + meta_q;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const long long t0 = (long long)blockIdx.x * NT;
+  const int blk = blockIdx.y;
+  const int g = min(blk * kPatWarps + warp, p.ngroups - 1);
+  const T* fb = reinterpret_cast<const T*>(p.fb);
+  const int nchunks = (p.nchan + CH - 1) / CH;
+  int err = 0;
+
+  auto stage = [&](int k, int b) {
+    const int c0 = k * CH;
+    const int nc = min(CH, p.nchan - c0);
+    // metadata: this warp's channels of the chunk, sorted into runs of one pattern
+    {
+      int pat = 0x10000 + lane;  // inactive lanes: a pattern of their own
+      int slot = 0;
+      unsigned pk = 0;
+      if (lane < nc) {
+        const int c = c0 + lane;
+        const long long a0 = (p.row0 + t0 + __ldg(p.bmin + (long long)blk * p.nchan + c)) & ~(long long)(VEC - 1);
+        int rel = (int)(p.row0 + t0 + __ldg(p.gbase + (long long)g * p.nchan + c) - a0);
+        if (rel < 0 || rel + NT + SMAX > LM) {  // cannot happen with a consistent plan
+          err |= kErrOffsetRange;
+          rel = 0;
+        }
+        slot = lane * LM + rel;
+        pk = __ldg(p.gpack + (long long)g * p.nchan + c);
+        pat = __ldg(p.gpat + (long long)g * p.nchan + c);
+      }
+      const unsigned same = __match_any_sync(0xffffffffu, pat);
+      const int leader = __ffs(same) - 1;
+      const bool lead = lane == leader && lane < nc;
+      const int cnt = __popc(same);
+      int incl = lead ? cnt : 0;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += y;
+      }
+      const int start_l = incl - (lead ? cnt : 0);
+      const int start = __shfl_sync(0xffffffffu, start_l, leader);
+      const unsigned below = (1u << lane) - 1u;
+      const int rank = __popc(same & below);
+      const int mb = (b * kPatWarps + warp) * CH;
+      const unsigned leads = __ballot_sync(0xffffffffu, lead);
+      if (lane < nc) {
+        s_slot[mb + start + rank] = slot;
+        s_pk[mb + start + rank] = pk;
+      }
+      if (lead) s_run[mb + __popc(leads & below)] = (pat & 0xFF) | (start << 8) | (cnt << 16);
+      if (lane == 0) s_nrun[b * kPatWarps + warp] = __popc(leads);
+    }
+    for (int cl = warp; cl < nc; cl += kPatWarps) {
+      const long long a = (p.row0 + t0 + __ldg(p.bmin + (long long)blk * p.nchan + c0 + cl)) & ~(long long)(VEC - 1);
+      const T* src = fb + (long long)(c0 + cl) * p.chan_stride;
+      int4* dst = tiles + ((long long)b * CH + cl) * LMQ;
+      const long long vend = p.row0 + p.nrows_valid;
+      for (int v = lane; v < LMQ; v += 32) {
+        const long long r = a + (long long)v * VEC;
+        int bytes = 0;
+        if (r >= 0 && r < vend) bytes = (int)(min((long long)VEC, vend - r) * (long long)sizeof(T));
+        const unsigned long long rr = (unsigned long long)(bytes ? r : 0) & (unsigned long long)p.row_mask;
+        cp_async16(dst + v, src + rr, bytes);
+      }
+    }
+    cp_async_commit();
+  };
+
+  float acc[D][TT];
+#pragma unroll
+  for (int j = 0; j < D; ++j)
+#pragma unroll
+    for (int i = 0; i < TT; ++i) acc[j][i] = 0.f;
+
+  stage(0, 0);
+  for (int k = 0; k < nchunks; ++k) {
+    cp_async_wait_all();
+    __syncthreads();
+    if (k + 1 < nchunks) stage(k + 1, (k + 1) & 1);
+    const int b = k & 1;
+    const T* tile = reinterpret_cast<const T*>(tiles + (long long)b * CH * LMQ);
+    const int mb = (b * kPatWarps + warp) * CH;
+    const int nrun = s_nrun[b * kPatWarps + warp];
+#pragma unroll 1
+    for (int r = 0; r < nrun; ++r) {
+      const int rd = s_run[mb + r];
+      const int s0 = (rd >> 8) & 0xFF;
+      pat_dispatch<T, D, TT, SMAX>(acc, rd & 0xFF, tile, s_slot + mb + s0, s_pk + mb + s0, rd >> 16, lane * TT);
+    }
+  }
+
+  // epilogue: out = sum / NCHANOUT (PIPE:1534) x scale; calcstats partials per (DM, time block)
+  const float fs = p.out_scale / (float)p.nchan;
+  const bool plain = p.out_scale == 1.f;
+  const float fn = (float)p.nchan;
+  const int gw = blk * kPatWarps + warp;
+#pragma unroll
+  for (int j = 0; j < D; ++j) {
+    const int d = gw * D + j;
+    if (d >= p.ndm) continue;  // warp-uniform
+    double s = 0.0, s2 = 0.0;
+    float mx = -INFINITY;
+    int arg = 0x7fffffff;
+    float* orow = p.out + (long long)d * p.out_stride;
+#pragma unroll
+    for (int i = 0; i < TT; ++i) {
+      const long long t = t0 + (long long)lane * TT + i;
+      if (t < p.nt_out) {
+        const float val = plain ? acc[j][i] / fn : acc[j][i] * fs;
+        orow[t] = val;
+        s += (double)val;
+        s2 += (double)val * (double)val;
+        if (val > mx) {
+          mx = val;
+          arg = (int)t;
+        }
+      }
+    }
+    s = wsum(s);
+    s2 = wsum(s2);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      const float omx = __shfl_xor_sync(0xffffffffu, mx, o);
+      const int oarg = __shfl_xor_sync(0xffffffffu, arg, o);
+      if (omx > mx || (omx == mx && oarg < arg)) {
+        mx = omx;
+        arg = oarg;
+      }
+    }
+    if (lane == 0 && p.part) {
+      DmPartial pq;
+      pq.s = s;
+      pq.s2 = s2;
+      pq.mx = mx;
+      pq.arg = arg;
+      p.part[(long long)blockIdx.x * p.ndm + d] = pq;
+    }
+  }
+  if (err && p.err) atomicOr(p.err, err);
+}
+
+}  // namespace vfrb

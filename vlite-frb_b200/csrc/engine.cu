@@ -1001,4 +1001,14 @@ const char* vfrb_stream_log(vfrb_plan* pl, int stream) {
   return pl->logtmp.c_str();
 }
 
+int vfrb_stream_tstart(vfrb_plan* pl, int stream, double* mjd) {
+  if (!pl || !mjd || stream < 0 || stream >= (int)pl->st.size()) return VFRB_ERR_ARG;
+  const StreamSt* s = pl->st[stream].get();
+  if (s->started) {
+    *mjd = s->tstart_mjd;
+    return VFRB_OK;
+  }
+  return s->reader_error ? s->reader_error : VFRB_PENDING;
+}
+
 }  // extern "C"

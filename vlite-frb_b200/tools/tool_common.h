@@ -1,0 +1,156 @@
+// Shared host code of the drop-in command-line tools (built on libvfrb's
+// plan API; see include/vfrb.h).
+#pragma once
+
+#include <sys/stat.h>
+#include <unistd.h>
+
+#include <chrono>
+#include <cstdarg>
+#include <cstdint>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "vfrb.h"
+
+namespace tool {
+
+inline bool eq(const char* a, const char* b) { return std::strcmp(a, b) == 0; }
+
+inline double now_s() {
+  return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+
+// The reference opens DM101.txt in the working directory, counts its lines and
+// reads one float per line with sscanf("%f") (PIPE:355-376, 420-431).
+inline int read_dm_list(const char* path, std::vector<float>& dms) {
+  FILE* f = std::fopen(path, "r");
+  if (!f) return -1;
+  char line[256];
+  int n = 0;
+  while (std::fgets(line, sizeof line, f)) ++n;
+  std::rewind(f);
+  dms.assign((size_t)n, 0.f);
+  for (int i = 0; i < n; ++i) {
+    if (!std::fgets(line, sizeof line, f)) break;
+    std::sscanf(line, "%f", &dms[(size_t)i]);
+  }
+  std::fclose(f);
+  return n;
+}
+
+inline bool file_exists(const char* p) { return access(p, F_OK) != -1; }
+
+inline bool write_all(FILE* f, const void* p, size_t n) { return n == 0 || std::fwrite(p, 1, n, f) == n; }
+
+// Byte source the tools read VDIF from: a file ("-" = standard input) or a
+// DADA-style ring named by its key (vfrb_dada_*).
+struct Source {
+  FILE* f = nullptr;
+  bool own = false;
+  vfrb_dada* ring = nullptr;
+  int timeout_ms = 300000;
+  bool failed = false;
+  bool open(const char* path) {
+    if (eq(path, "-")) {
+      f = stdin;
+      return true;
+    }
+    f = std::fopen(path, "rb");
+    own = f != nullptr;
+    return f != nullptr;
+  }
+  // ipcio_connect + ipcio_open('R'): waits (bounded) for the writer's ring
+  bool connect(uint32_t key, int wait_ms = 30000) {
+    const double t0 = now_s();
+    while (vfrb_dada_connect(key, &ring) != VFRB_OK) {
+      if ((now_s() - t0) * 1e3 > wait_ms) return false;
+      usleep(20000);
+    }
+    return true;
+  }
+  size_t read(void* buf, size_t n) {
+    if (ring) {
+      const int64_t k = vfrb_dada_read(ring, buf, n, timeout_ms);
+      if (k < 0) {
+        failed = true;
+        return 0;
+      }
+      return (size_t)k;
+    }
+    return std::fread(buf, 1, n, f);
+  }
+  ~Source() {
+    if (own) std::fclose(f);
+    if (ring) vfrb_dada_close(ring);
+  }
+};
+
+// Feeds a source through a plan, calling on_result for every completed
+// result and on_start once the reader has found its first frame pair.
+// Returns 0, or the reference's exit code for the failure (2).
+template <typename OnStart, typename OnResult>
+int run_stream(vfrb_plan* plan, Source& src, FILE* log, OnStart on_start, OnResult on_result) {
+  std::vector<uint8_t> buf((size_t)64 << 20);
+  bool started = false;
+  auto drain = [&](int wait) -> int {
+    for (;;) {
+      vfrb_result r;
+      const int st = vfrb_poll(plan, &r, wait);
+      if (st == VFRB_PENDING || st == VFRB_EOD) return st;
+      if (st != VFRB_OK) return st;
+      on_result(r);
+    }
+  };
+  auto check_start = [&]() {
+    if (started) return;
+    double mjd = 0.0;
+    if (vfrb_stream_tstart(plan, 0, &mjd) == VFRB_OK) {
+      started = true;
+      on_start(mjd);
+    }
+  };
+  for (;;) {
+    const size_t n = src.read(buf.data(), buf.size());
+    if (n == 0) break;
+    int st = vfrb_push_frames(plan, 0, buf.data(), n);
+    if (st != VFRB_OK) {
+      std::fprintf(log, "%s\n", vfrb_stream_log(plan, 0));
+      std::fprintf(log, "processing stopped: %s\n", vfrb_strerror(st));
+      return 2;
+    }
+    check_start();
+    st = drain(0);
+    if (st != VFRB_PENDING && st != VFRB_EOD) {
+      std::fprintf(log, "processing stopped: %s\n", vfrb_strerror(st));
+      return 2;
+    }
+  }
+  if (src.failed) {
+    std::fprintf(log, "no data from the input ring for %d ms\n", src.timeout_ms);
+    return 2;
+  }
+  int st = vfrb_push_frames(plan, 0, nullptr, 0);  // end of data (FLAGEOF / FLAGEODADA)
+  check_start();
+  if (st != VFRB_OK && st != VFRB_EOD) {
+    std::fprintf(log, "%s\n", vfrb_stream_log(plan, 0));
+    std::fprintf(log, "processing stopped: %s\n", vfrb_strerror(st));
+    return 2;
+  }
+  st = drain(1);
+  if (st != VFRB_EOD && st != VFRB_PENDING) {
+    std::fprintf(log, "processing stopped: %s\n", vfrb_strerror(st));
+    return 2;
+  }
+  std::fputs(vfrb_stream_log(plan, 0), log);
+  if (!started) {
+    std::fprintf(log, "initframe01 returned in error!\n");
+    return 2;
+  }
+  return 0;
+}
+
+}  // namespace tool
