@@ -360,17 +360,26 @@ def gpu_reference_baseline(vf, sample_bundles=32):
 
 
 # --------------------------------------------------------------------------- distributed helpers
-def dist_init(n):
+def dist_init(n, backend="nccl", timeout_s=120):
+    """One process per GPU (torchrun env).  The only collective on the path is
+    the max-over-ranks of the step time; a short process-group timeout makes a
+    rank that left end the others' next collective with an error."""
     if n <= 1 and "RANK" not in os.environ:
         return None
+    import datetime
     import torch
     import torch.distributed as d
     rank = int(os.environ.get("RANK", 0))
     local = int(os.environ.get("LOCAL_RANK", 0))
-    torch.cuda.set_device(local)
-    import datetime
-    d.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
-    return dict(rank=rank, world=d.get_world_size(), local=local)
+    if backend == "nccl":
+        torch.cuda.set_device(local)
+    d.init_process_group(backend, timeout=datetime.timedelta(seconds=timeout_s))
+    return dict(rank=rank, world=d.get_world_size(), local=local, device="cuda" if backend == "nccl" else "cpu")
+
+
+def stream_seed(rank):
+    """Each rank synthesises and processes its own independent stream (antenna)."""
+    return SEED + 1000 * rank
 
 
 def dist_barrier(dist):
@@ -384,7 +393,7 @@ def dist_max(dist, v):
         return v
     import torch
     import torch.distributed as d
-    t = torch.tensor([v], dtype=torch.float64, device="cuda")
+    t = torch.tensor([v], dtype=torch.float64, device=dist.get("device", "cuda"))
     d.all_reduce(t, op=d.ReduceOp.MAX)
     return float(t.item())
 
@@ -436,7 +445,7 @@ def main():
     world = dist["world"] if dist else 1
     dev = torch.device("cuda")
     # each rank processes its own independent stream (antenna): weak scaling, no collective on the data path
-    spec = synth.StreamSpec(duration=args.duration, seed=SEED + 1000 * rank,
+    spec = synth.StreamSpec(duration=args.duration, seed=stream_seed(rank),
                             pulses=[synth.Pulse(*p) for p in pulses(duration=args.duration)])
     t_gen = time.perf_counter()
     frames = synth.make_vdif(spec, device=dev)

@@ -1,0 +1,86 @@
+"""The N>1 path of bench.py on CPU: two ranks as separate processes over
+gloo (world size 2, 127.0.0.1).  Each rank owns an independent stream (its
+own seed, no data collective); the only collective is the max-over-ranks of
+the step time.  A rank that leaves before the collective makes the other
+rank's next collective end with an error within the short process-group
+timeout instead of hanging (failure detected on the host)."""
+import importlib.util
+import os
+import socket
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def _bench():
+    spec = importlib.util.spec_from_file_location("vfrb_bench", os.path.join(ROOT, "bench.py"))
+    m = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(m)
+    return m
+
+
+def _free_port():
+    s = socket.socket()
+    s.bind(("127.0.0.1", 0))
+    p = s.getsockname()[1]
+    s.close()
+    return p
+
+
+def _worker(rank, world, port, q, leave_rank):
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port), RANK=str(rank), WORLD_SIZE=str(world),
+                      LOCAL_RANK=str(rank))
+    b = _bench()
+    dist = b.dist_init(world, backend="gloo", timeout_s=5)
+    try:
+        if rank == leave_rank:
+            q.put((rank, "left", None, None))
+            return  # leaves between steps, with nothing in flight
+        b.dist_barrier(dist)
+        v = b.dist_max(dist, 10.0 + rank)
+        q.put((rank, "ok", v, b.stream_seed(rank)))
+    except Exception as e:  # noqa: BLE001
+        q.put((rank, "err", type(e).__name__, None))
+    finally:
+        try:
+            import torch.distributed as d
+            if leave_rank < 0:
+                d.destroy_process_group()
+        except Exception:  # noqa: BLE001
+            pass
+
+
+def _run(world, leave_rank, timeout=60):
+    import torch.multiprocessing as mp
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    ps = [ctx.Process(target=_worker, args=(r, world, port, q, leave_rank)) for r in range(world)]
+    for p in ps:
+        p.start()
+    out = {}
+    try:
+        for _ in range(world):
+            r = q.get(timeout=timeout)
+            out[r[0]] = r[1:]
+    finally:
+        for p in ps:
+            p.join(timeout=30)
+            if p.is_alive():
+                p.kill()
+                p.join()
+    return out
+
+
+def test_two_ranks_max_time_and_independent_streams():
+    out = _run(2, -1)
+    assert out[0][0] == "ok" and out[1][0] == "ok", out
+    assert out[0][1] == out[1][1] == 11.0  # max over ranks on every rank
+    assert out[0][2] != out[1][2]  # each rank synthesises its own stream
+
+
+def test_rank_leaving_is_detected_by_timeout():
+    out = _run(2, 1)
+    assert out[1][0] == "left"
+    assert out[0][0] == "err", out  # the collective ends with an error, no hang

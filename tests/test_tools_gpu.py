@@ -38,7 +38,7 @@ def _close(got, ref, tol, what):
     assert e <= tol, (what, e)
 
 
-def test_pipe_tool_outputs(O, co, tmp_path):
+def test_pipe_tool_outputs(vf, O, co, tmp_path):
     from vlite_frb_b200 import synth
     nave, maxtime = 2, 0.2
     dms = np.arange(0, 5.5, 0.5, dtype=np.float32)
@@ -74,7 +74,7 @@ def test_pipe_tool_outputs(O, co, tmp_path):
     _close(fil, bp, 5e-5, "nohead.fil (block 4)")
 
 
-def test_pipe_tool_short_input_and_bad_args(tmp_path):
+def test_pipe_tool_short_input_and_bad_args(vf, tmp_path):
     from vlite_frb_b200 import synth
     exe = _tool("vdifFILE2dedisp_PIPELINE")
     assert subprocess.run([exe], cwd=tmp_path, capture_output=True).returncode == 1
@@ -94,7 +94,7 @@ def test_pipe_tool_short_input_and_bad_args(tmp_path):
     assert (tmp_path / "o.head").stat().st_size > 0
 
 
-def test_stats_tool_file_and_ring(O, co, tmp_path):
+def test_stats_tool_file_and_ring(vf, O, co, tmp_path):
     """vdifDADA2stats: the .stats file holds, per block, CHANAVE, CHANSIGMA and
     CHANOUTLIER [NSTATBLKS][NCHANOUT]; reading the same bytes from the ring
     (fed by vfrb_dada_write) gives an identical file."""
@@ -135,7 +135,7 @@ def test_stats_tool_file_and_ring(O, co, tmp_path):
     assert (tmp_path / "k.stats").read_bytes() == (tmp_path / "f.stats").read_bytes()
 
 
-def test_timeseries_tool_outputs(O, co, tmp_path):
+def test_timeseries_tool_outputs(vf, O, co, tmp_path):
     """vdifDADA2timeseries: DM 0 and DM 119.3 channel-mean and sigma series
     appended per block; the .inf headers (written at the end with -infatend)
     equal the reference's writeprestoheader text."""

@@ -1,11 +1,11 @@
 // K1: fused channeliser for sm_100a.
 //
 // A persistent CTA (512 threads, one per SM) produces filterbank rows in turn;
-// each row is: NAVE consecutive 12500-sample windows
-// of both polarisations.  Per window the two real 8-bit streams are packed
-// into one complex sequence z[n] = (x0[n]-128) + i (x1[n]-128) and transformed
-// by a hand-written 12500-point mixed-radix Stockham FFT (radices 25, 25, 20)
-// that lives entirely in shared memory (100 kB).  Because
+// each row is NAVE consecutive 12500-sample windows of both polarisations.
+// Per window the two real 8-bit streams are packed into one complex sequence
+// z[n] = (x0[n]-128) + i (x1[n]-128) and transformed by a hand-written
+// 12500-point mixed-radix Stockham FFT (radices 25, 25, 20) that lives
+// entirely in shared memory (100 kB).  Because
 //   |X0[k]|^2 + |X1[k]|^2 = (|Z[k]|^2 + |Z[N-k]|^2) / 2,
 // detection, the polarisation sum, /NFREQ, the NAVE average and the NSKIP
 // channel slice are an epilogue on Z.  The -128 offset only changes bin 0,
@@ -13,6 +13,13 @@
 // well conditioned.  This replaces convertarray, cufftExecR2C, sumpower,
 // avepower and the per-row D2D copies of PIPE:574-632 (STATS:377-405,
 // TS:603-636).
+//
+// Input staging: the raw bytes of the NEXT window (2 x 12500) are copied
+// from the frame ring into a second shared-memory byte buffer with 4-byte
+// cp.async while the current window is transformed, so the global-memory
+// latency is hidden behind the FFT; the byte -> float conversion is fused
+// into the first pass's loads.  Gap frames (slot -1) are zero-filled by the
+// copy itself.
 #include "vfrb_common.cuh"
 #include "dft_codelets.cuh"
 
@@ -29,22 +36,33 @@ constexpr int kM3 = kFftN / kR3;  // 625 butterflies in pass 3
 constexpr int kNs2 = kR1;         // 25
 constexpr int kNs3 = kR1 * kR2;   // 625
 
-// Twiddles, computed on the host in double precision and rounded to float
-// (row r = 0 is all ones and is not stored):
-//   g_tw2[r-1][m] = W_625^(m r),   m < 25,  1 <= r < 25   (pass 2, Ns = 25)
-//   g_tw3[r-1][m] = W_12500^(m r), m < 625, 1 <= r < 20   (pass 3, Ns = 625)
-// Each CTA copies both tables into shared memory once.
+// Twiddles, computed on the host in double precision and rounded to float:
+//   g_tw2[r-1][m] = W_625^(m r), m < 25, 1 <= r < 25   (pass 2, Ns = 25)
+//   pass 3 needs W_12500^q for q = m r < 12500 (m < 625, r < 20); with
+//   q = 125 h + l it is g_thi[h] * g_tlo[l], g_thi[h] = W_100^h (h < 100),
+//   g_tlo[l] = W_12500^l (l < 125): 1.8 kB instead of a 95 kB table.
+// Each CTA copies the tables into shared memory once.
 constexpr int kTw2 = (kR2 - 1) * kNs2;  // 600
-constexpr int kTw3 = (kR3 - 1) * kNs3;  // 11875
+constexpr int kThi = 100, kTlo = 125;
+// tlo[l] is stored at l + l/16: for r a multiple of 2..16 the half-warp's
+// indices (j r) mod 125 are spaced by r, which would put up to 16 of them in
+// one bank; the skew spreads them
+constexpr int kTloPad = kTlo + (kTlo - 1) / 16 + 1;  // 133
+__host__ __device__ constexpr int tlo_at(int l) { return l + (l >> 4); }
 constexpr int kAccFloats = kFftN / 2 + 2;  // 6252 >= any NCHANOUT
+constexpr int kStage = 12512;              // one pol's window bytes, padded to 16
 __device__ float2 g_tw2[kTw2];
-__device__ float2 g_tw3[kTw3];
-// shared-memory layout (bytes): Z | tw3 | tw2 | acc
+__device__ float2 g_thi[kThi];
+__device__ float2 g_tlo[kTloPad];
+// shared-memory layout (bytes): Z | stage[2 buffers][2 pols] | tw2 | thi | tlo | acc
 constexpr size_t kSmZ = sizeof(float2) * kFftN;
-constexpr size_t kSmTw3 = sizeof(float2) * kTw3;
+constexpr size_t kSmStage = (size_t)4 * kStage;
 constexpr size_t kSmTw2 = sizeof(float2) * kTw2;
-constexpr size_t kSmem = kSmZ + kSmTw3 + kSmTw2 + sizeof(float) * kAccFloats;
+constexpr size_t kSmThi = sizeof(float2) * kThi;
+constexpr size_t kSmTlo = sizeof(float2) * ((kTloPad + 1) / 2 * 2);
+constexpr size_t kSmem = kSmZ + kSmStage + kSmTw2 + kSmThi + kSmTlo + sizeof(float) * kAccFloats;
 static_assert(kSmem <= 227 * 1024, "channeliser shared memory");
+static_assert(kSmZ % 16 == 0 && kSmStage % 16 == 0 && kStage % 16 == 0, "16-byte aligned regions");
 
 static std::mutex g_tw_mu;
 static bool g_tw_ready[64];
@@ -54,19 +72,23 @@ static int ensure_twiddles() {
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return VFRB_ERR_CUDA;
   std::lock_guard<std::mutex> lk(g_tw_mu);
   if (g_tw_ready[dev]) return VFRB_OK;
-  static float2 h2[kTw2], h3[kTw3];
+  static float2 h2[kTw2], hh[kThi], hl[kTloPad];
   for (int r = 1; r < kR2; ++r)
     for (int m = 0; m < kNs2; ++m) {
-      double a = -2.0 * M_PI * (double)((m * r) % 625) / 625.0;
+      const double a = -2.0 * M_PI * (double)((m * r) % 625) / 625.0;
       h2[(r - 1) * kNs2 + m] = make_float2((float)cos(a), (float)sin(a));
     }
-  for (int r = 1; r < kR3; ++r)
-    for (int m = 0; m < kNs3; ++m) {
-      double a = -2.0 * M_PI * (double)((m * r) % kFftN) / (double)kFftN;
-      h3[(r - 1) * kNs3 + m] = make_float2((float)cos(a), (float)sin(a));
-    }
+  for (int h = 0; h < kThi; ++h) {
+    const double a = -2.0 * M_PI * (double)h / 100.0;
+    hh[h] = make_float2((float)cos(a), (float)sin(a));
+  }
+  for (int l = 0; l < kTlo; ++l) {
+    const double a = -2.0 * M_PI * (double)l / (double)kFftN;
+    hl[tlo_at(l)] = make_float2((float)cos(a), (float)sin(a));
+  }
   if (cudaMemcpyToSymbol(g_tw2, h2, sizeof(h2)) != cudaSuccess) return VFRB_ERR_CUDA;
-  if (cudaMemcpyToSymbol(g_tw3, h3, sizeof(h3)) != cudaSuccess) return VFRB_ERR_CUDA;
+  if (cudaMemcpyToSymbol(g_thi, hh, sizeof(hh)) != cudaSuccess) return VFRB_ERR_CUDA;
+  if (cudaMemcpyToSymbol(g_tlo, hl, sizeof(hl)) != cudaSuccess) return VFRB_ERR_CUDA;
   g_tw_ready[dev] = true;
   return VFRB_OK;
 }
@@ -75,33 +97,40 @@ __device__ __forceinline__ float2 cmul(float2 a, float2 b) {
   return make_float2(fmaf(a.x, b.x, -a.y * b.y), fmaf(a.x, b.y, a.y * b.x));
 }
 
-// Load one 12500-sample window of both pols into Z as (x0-128) + i(x1-128).
-// ALIGNED: every 4-sample group lies inside one payload at a 4-byte boundary
-// (true whenever sample0 and TWONCHAN are multiples of 4).
+__device__ __forceinline__ void cp_async4(void* smem_dst, const void* gsrc, int src_bytes) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(smem_dst);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(d), "l"(gsrc), "r"(src_bytes));
+}
+__device__ __forceinline__ void cp_async_commit_k1() { asm volatile("cp.async.commit_group;\n" ::); }
+__device__ __forceinline__ void cp_async_wait_1() { asm volatile("cp.async.wait_group 1;\n" ::); }
+
+// Stage the raw bytes of one 12500-sample window of both pols (stream
+// positions pos0 ..) into st0 / st1.  ALIGNED (sample0 % 4 == 0): 4-byte
+// asynchronous copies, each inside one payload; otherwise synchronous byte
+// loads.  Positions outside the slot table and misaligned payloads set
+// kErrSlotRange and read as zero bytes.
 template <bool ALIGNED>
-__device__ __forceinline__ void load_window(float2* __restrict__ Z, const vfrb_chan_args& a, long long pos0,
-                                            int& err) {
+__device__ __forceinline__ void stage_window(unsigned char* __restrict__ st0, unsigned char* __restrict__ st1,
+                                             const vfrb_chan_args& a, long long pos0, int& err) {
   const int tid = threadIdx.x;
   if (ALIGNED) {
     for (int g = tid; g < kFftN / 4; g += kThreads) {
       const long long pos = pos0 + 4LL * g;
       const long long slot = pos / kDataLen;
       const int off = (int)(pos - slot * kDataLen);
-      uchar4 b0 = make_uchar4(0, 0, 0, 0), b1 = b0;
+      long long s0 = -1, s1 = -1;
       if (pos < 0 || slot >= a.nslots) {
         err |= kErrSlotRange;
       } else {
-        const long long s0 = __ldg(a.slots0 + slot), s1 = __ldg(a.slots1 + slot);
-        if (((s0 | s1) & 3) != 0 && s0 >= 0 && s1 >= 0) {
-          err |= kErrSlotRange;  // payloads must start on a 4-byte boundary
-        } else {
-          if (s0 >= 0 && (s0 & 3) == 0) b0 = __ldg(reinterpret_cast<const uchar4*>(a.frames + s0 + off));
-          if (s1 >= 0 && (s1 & 3) == 0) b1 = __ldg(reinterpret_cast<const uchar4*>(a.frames + s1 + off));
+        s0 = __ldg(a.slots0 + slot);
+        s1 = __ldg(a.slots1 + slot);
+        if ((s0 >= 0 && (s0 & 3)) || (s1 >= 0 && (s1 & 3))) {  // payloads must start on a 4-byte boundary
+          err |= kErrSlotRange;
+          s0 = s1 = -1;
         }
       }
-      float4* z4 = reinterpret_cast<float4*>(Z + 4 * g);
-      z4[0] = make_float4((float)b0.x - 128.f, (float)b1.x - 128.f, (float)b0.y - 128.f, (float)b1.y - 128.f);
-      z4[1] = make_float4((float)b0.z - 128.f, (float)b1.z - 128.f, (float)b0.w - 128.f, (float)b1.w - 128.f);
+      cp_async4(st0 + 4 * g, s0 >= 0 ? a.frames + s0 + off : a.frames, s0 >= 0 ? 4 : 0);
+      cp_async4(st1 + 4 * g, s1 >= 0 ? a.frames + s1 + off : a.frames, s1 >= 0 ? 4 : 0);
     }
   } else {
     for (int n = tid; n < kFftN; n += kThreads) {
@@ -116,32 +145,31 @@ __device__ __forceinline__ void load_window(float2* __restrict__ Z, const vfrb_c
         if (s0 >= 0) v0 = __ldg(a.frames + s0 + off);
         if (s1 >= 0) v1 = __ldg(a.frames + s1 + off);
       }
-      Z[n] = make_float2((float)v0 - 128.f, (float)v1 - 128.f);
+      st0[n] = v0;
+      st1[n] = v1;
     }
   }
 }
 
-// In-place 12500-point forward FFT of Z (natural order in and out).
+// 12500-point forward FFT of the staged window into Z (natural order out).
 // Stockham passes: data1[(j/Ns)*Ns*R + j%Ns + r*Ns] = DFT_R(data0[j + r*N/R] * W^(r*(j%Ns)*N/(Ns*R))).
-// Each pass holds its butterfly inputs in registers across a barrier, so one
-// buffer suffices.
-__device__ __forceinline__ void fft12500(float2* __restrict__ Z, const float2* __restrict__ tw2,
-                                         const float2* __restrict__ tw3) {
+// Pass 1 reads the staged bytes (not Z), so it needs no barrier between its
+// reads and writes; passes 2 and 3 hold their inputs in registers across
+// one barrier, so one Z buffer suffices.
+__device__ __forceinline__ void fft12500(float2* __restrict__ Z, const unsigned char* __restrict__ st0,
+                                         const unsigned char* __restrict__ st1, const float2* __restrict__ tw2,
+                                         const float2* __restrict__ thi, const float2* __restrict__ tlo) {
   const int tid = threadIdx.x;
-  {  // pass 1: R = 25, Ns = 1 (no twiddles); writes are stride 25 (odd -> no bank conflicts)
+  if (tid < kM1) {  // pass 1: R = 25, Ns = 1 (no twiddles); writes stride 25 (odd -> no bank conflicts)
     float2 v[kR1];
-    if (tid < kM1) {
 #pragma unroll
-      for (int r = 0; r < kR1; ++r) v[r] = Z[tid + r * kM1];
-      dft25(v);
-    }
-    __syncthreads();
-    if (tid < kM1) {
+    for (int r = 0; r < kR1; ++r)
+      v[r] = make_float2((float)st0[tid + r * kM1] - 128.f, (float)st1[tid + r * kM1] - 128.f);
+    dft25(v);
 #pragma unroll
-      for (int r = 0; r < kR1; ++r) Z[tid * kR1 + r] = v[dft25_pos(r)];
-    }
-    __syncthreads();
+    for (int r = 0; r < kR1; ++r) Z[tid * kR1 + r] = v[dft25_pos(r)];
   }
+  __syncthreads();
   {  // pass 2: R = 25, Ns = 25
     float2 v[kR2];
     const int m = tid % kNs2;
@@ -167,8 +195,19 @@ __device__ __forceinline__ void fft12500(float2* __restrict__ Z, const float2* _
       float2 u[kR3];
 #pragma unroll
       for (int r = 0; r < kR3; ++r) u[r] = Z[j + r * kM3];
+      // twiddle W^(j r) = thi[h] * tlo[l] with j r = 125 h + l, stepped in r
+      const int h1 = j / kTlo, l1 = j - kTlo * h1;
+      int h = 0, l = 0;
 #pragma unroll
-      for (int r = 1; r < kR3; ++r) u[r] = cmul(u[r], tw3[(r - 1) * kNs3 + j]);
+      for (int r = 1; r < kR3; ++r) {
+        l += l1;
+        h += h1;
+        if (l >= kTlo) {
+          l -= kTlo;
+          ++h;
+        }
+        u[r] = cmul(u[r], cmul(thi[h], tlo[tlo_at(l)]));
+      }
       dft20(u);
 #pragma unroll
       for (int r = 0; r < kR3; ++r) Z[j + r * kNs3] = u[dft20_pos(r)];
@@ -182,38 +221,60 @@ __global__ void __launch_bounds__(kThreads, 1) k_channelise(const vfrb_chan_args
   extern __shared__ float4 smem_f4[];
   unsigned char* sm = reinterpret_cast<unsigned char*>(smem_f4);
   float2* Z = reinterpret_cast<float2*>(sm);
-  float2* tw3 = reinterpret_cast<float2*>(sm + kSmZ);
-  float2* tw2 = reinterpret_cast<float2*>(sm + kSmZ + kSmTw3);
+  unsigned char* stage = sm + kSmZ;  // [2 buffers][2 pols][kStage]
+  float2* tw2 = reinterpret_cast<float2*>(sm + kSmZ + kSmStage);
+  float2* thi = reinterpret_cast<float2*>(sm + kSmZ + kSmStage + kSmTw2);
+  float2* tlo = reinterpret_cast<float2*>(sm + kSmZ + kSmStage + kSmTw2 + kSmThi);
   // per-bin power accumulators live in shared memory (each thread owns the
   // same bins in every window), keeping registers for the butterflies
-  float* acc = reinterpret_cast<float*>(sm + kSmZ + kSmTw3 + kSmTw2);
+  float* acc = reinterpret_cast<float*>(sm + kSmZ + kSmStage + kSmTw2 + kSmThi + kSmTlo);
   const int tid = threadIdx.x;
   int err = 0;
-  for (int i = tid; i < kTw3; i += kThreads) tw3[i] = g_tw3[i];
   for (int i = tid; i < kTw2; i += kThreads) tw2[i] = g_tw2[i];
+  for (int i = tid; i < kThi; i += kThreads) thi[i] = g_thi[i];
+  for (int i = tid; i < kTloPad; i += kThreads) tlo[i] = g_tlo[i];
+  for (int c = tid; c < a.nchanout; c += kThreads) acc[c] = 0.f;
   const float scale = 1.0f / (2.0f * (float)a.nfreq * (float)a.nave);
 
-  // persistent CTAs: one per SM, striding over the rows
-  for (long long row = blockIdx.x; row < a.nrows; row += gridDim.x) {
-    for (int c = tid; c < a.nchanout; c += kThreads) acc[c] = 0.f;
-    for (int w = 0; w < a.nave; ++w) {
-      const long long pos0 = a.sample0 + (row * a.nave + w) * (long long)kFftN;
-      load_window<ALIGNED>(Z, a, pos0, err);
-      __syncthreads();
-      fft12500(Z, tw2, tw3);
-      // epilogue: |Z_k|^2 + |Z_{N-k}|^2 for the selected bins
-      for (int c = tid; c < a.nchanout; c += kThreads) {
-        const int k = a.nskip + c;
-        const float2 z1 = Z[k];
-        const float2 z2 = Z[kFftN - k];
-        acc[c] += fmaf(z1.x, z1.x, z1.y * z1.y) + fmaf(z2.x, z2.x, z2.y * z2.y);
-      }
-      __syncthreads();
-    }
-    // (|X0|^2 + |X1|^2)/NFREQ averaged over NAVE spectra (PIPE:1296, 1310)
+  // persistent CTAs: one per SM; this CTA's windows are (row, w) for rows
+  // blockIdx.x + k*gridDim.x, w < NAVE, in that order
+  const long long nrows_cta = (a.nrows - blockIdx.x + gridDim.x - 1) / gridDim.x;
+  const long long nwin = nrows_cta * a.nave;
+  auto win_pos = [&](long long i) {
+    const long long row = blockIdx.x + (i / a.nave) * gridDim.x;
+    return a.sample0 + (row * a.nave + i % a.nave) * (long long)kFftN;
+  };
+  if (nwin > 0) stage_window<ALIGNED>(stage, stage + kStage, a, win_pos(0), err);
+  cp_async_commit_k1();
+  for (long long i = 0; i < nwin; ++i) {
+    unsigned char* cur = stage + (size_t)(i & 1) * 2 * kStage;
+    unsigned char* nxt = stage + (size_t)((i + 1) & 1) * 2 * kStage;
+    // the buffer of window i+1 was last read by pass 1 of window i-1, which
+    // every thread has left (barriers inside fft12500)
+    if (i + 1 < nwin) stage_window<ALIGNED>(nxt, nxt + kStage, a, win_pos(i + 1), err);
+    cp_async_commit_k1();
+    cp_async_wait_1();  // this thread's copies of window i have landed
+    __syncthreads();    // ... and everybody else's
+    fft12500(Z, cur, cur + kStage, tw2, thi, tlo);
+    // epilogue: |Z_k|^2 + |Z_{N-k}|^2 for the selected bins
+    const bool last = (i % a.nave) == a.nave - 1;
+    const long long row = blockIdx.x + (i / a.nave) * gridDim.x;
     const unsigned long long orow = (unsigned long long)(a.out_row0 + row) & (unsigned long long)a.out_row_mask;
     float* dst = a.out + (long long)orow * a.out_row_stride;
-    for (int c = tid; c < a.nchanout; c += kThreads) dst[c] = acc[c] * scale;
+    for (int c = tid; c < a.nchanout; c += kThreads) {
+      const int k = a.nskip + c;
+      const float2 z1 = Z[k];
+      const float2 z2 = Z[kFftN - k];
+      const float v = acc[c] + (fmaf(z1.x, z1.x, z1.y * z1.y) + fmaf(z2.x, z2.x, z2.y * z2.y));
+      if (last) {
+        // (|X0|^2 + |X1|^2)/NFREQ averaged over NAVE spectra (PIPE:1296, 1310)
+        dst[c] = v * scale;
+        acc[c] = 0.f;
+      } else {
+        acc[c] = v;
+      }
+    }
+    __syncthreads();  // Z is rewritten by the next window's pass 1
   }
   if (err && a.d_err) atomicOr(a.d_err, err);
 }

@@ -58,7 +58,7 @@ static double now_ms() {
   } while (0)
 
 constexpr int kStash = 1024;   // gap-revealing frames kept aside per stream
-constexpr int kSlotBufs = 4;   // rotating slot-table uploads in flight
+constexpr int kSlotBufs = 32;  // rotating slot-table uploads in flight (host runs ahead of the GPU)
 constexpr int kStageBufs = 2;  // rotating staging buffers for pageable input
 
 static unsigned long long pow2_at_least(unsigned long long v) {
@@ -123,6 +123,14 @@ struct StreamSt {
   cudaStream_t cs = nullptr;   // compute
   cudaStream_t xs = nullptr;   // host-to-device copies
   cudaEvent_t ev_copied = nullptr, ev_consumed = nullptr;
+  // Release events: one per channeliser launch, with the oldest frame any
+  // later work still reads (frames below it are free once the event has
+  // completed).  A copy into the ring waits only for the launch that freed
+  // the slots it overwrites, so copies run ahead of the compute stream.
+  static constexpr int kRelEv = 32;
+  cudaEvent_t rel_ev[kRelEv] = {};
+  int64_t rel_after[kRelEv] = {};
+  int rel_head = 0, rel_n = 0;
   std::unique_ptr<PairReader> reader;
   std::vector<uint8_t> part;   // bytes of an incomplete frame
   uint8_t* d_frames = nullptr; // frame ring followed by the stash
@@ -309,11 +317,15 @@ inline int64_t entry_offset(const StreamSt* s, int64_t v) {
 
 int64_t npairs(const StreamSt* s) { return s->ebase + (int64_t)(s->e0.size() - s->ehead); }
 
+int64_t oldest_ref(const StreamSt* s);
+
 void consume_entries(StreamSt* s, int64_t first_needed) {
   while (s->ebase < first_needed && s->ehead < s->e0.size()) {
     ++s->ehead;
     ++s->ebase;
   }
+  // the newest channeliser launch consumed these entries
+  if (s->rel_n > 0) s->rel_after[(s->rel_head + s->rel_n - 1) % StreamSt::kRelEv] = oldest_ref(s);
   if (s->ehead > 65536 && s->ehead * 2 > s->e0.size()) {
     s->e0.erase(s->e0.begin(), s->e0.begin() + (long)s->ehead);
     s->e1.erase(s->e1.begin(), s->e1.begin() + (long)s->ehead);
@@ -334,7 +346,7 @@ int launch_rows(vfrb_plan* pl, StreamSt* s, int64_t row_first, int64_t nrows, fl
   if (n > s->slots_cap || e_lo < s->ebase || e_hi > npairs(s)) return VFRB_ERR;
   SlotBuf& b = s->sb[s->sb_i];
   s->sb_i = (s->sb_i + 1) % kSlotBufs;
-  CK(cudaEventSynchronize(b.ev));  // the upload from this buffer four launches ago is done
+  CK(cudaEventSynchronize(b.ev));  // the upload from this buffer kSlotBufs launches ago is done
   for (int64_t i = 0; i < n; ++i) {
     const size_t k = s->ehead + (size_t)(e_lo - s->ebase + i);
     b.h[i] = entry_offset(s, s->e0[k]);
@@ -362,6 +374,14 @@ int launch_rows(vfrb_plan* pl, StreamSt* s, int64_t row_first, int64_t nrows, fl
   a.d_err = s->d_err;
   ST(launch_channelise(a, s->cs));
   CK(cudaEventRecord(s->ev_consumed, s->cs));
+  if (s->rel_n == StreamSt::kRelEv) {  // drop the oldest: later copies wait on newer (later) launches
+    s->rel_head = (s->rel_head + 1) % StreamSt::kRelEv;
+    --s->rel_n;
+  }
+  const int k = (s->rel_head + s->rel_n) % StreamSt::kRelEv;
+  CK(cudaEventRecord(s->rel_ev[k], s->cs));
+  s->rel_after[k] = INT64_MIN;  // set when this launch's entries are consumed
+  ++s->rel_n;
   return VFRB_OK;
 }
 
@@ -646,7 +666,22 @@ int feed_frames(vfrb_plan* pl, StreamSt* s, const uint8_t* host, int64_t nf, boo
       ST(process(pl, s, false));
       if (oldest_ref(s) < s->frames_in + nb - s->ring_frames) return VFRB_ERR_NOMEM;  // ring too small
     }
-    CK(cudaStreamWaitEvent(s->xs, s->ev_consumed, 0));
+    // the ring slots of this batch held frames below X; wait for the first
+    // channeliser launch after which none of them is read again
+    const int64_t X = s->frames_in + nb - s->ring_frames;
+    if (X > 0) {
+      cudaEvent_t wait_ev = s->ev_consumed;  // the latest launch, if no recorded one suffices
+      while (s->rel_n > 0) {
+        const int k = s->rel_head;
+        if (s->rel_after[k] >= X) {
+          wait_ev = s->rel_ev[k];
+          break;
+        }
+        s->rel_head = (s->rel_head + 1) % StreamSt::kRelEv;  // frees too little now, and X only grows
+        --s->rel_n;
+      }
+      CK(cudaStreamWaitEvent(s->xs, wait_ev, 0));
+    }
     const uint8_t* from = src;
     if (!pinned) {
       const int k = s->stage_i;
@@ -672,7 +707,9 @@ int feed_frames(vfrb_plan* pl, StreamSt* s, const uint8_t* host, int64_t nf, boo
     }
     CK(cudaEventRecord(s->ev_copied, s->xs));
     CK(cudaStreamWaitEvent(s->cs, s->ev_copied, 0));
-    for (int64_t i = 0; i < nb; ++i) {
+    // in-order pairs go straight to pair entries; the rest through the queue
+    int64_t i = (int64_t)s->reader->run_fast(src, s->frames_in, (size_t)nb, s->e0, s->e1);
+    for (; i < nb; ++i) {
       QFrame q;
       vfrb_decode_header(src + i * kFrameLen, &q.h);
       q.payload = s->frames_in + i;
@@ -713,6 +750,7 @@ int create_stream(vfrb_plan* pl, int id, int64_t ring_frames, int64_t R1, int64_
   pl->streams.push_back(s->xs);
   ST(mkevent(pl, &s->ev_copied));
   ST(mkevent(pl, &s->ev_consumed));
+  for (auto& e : s->rel_ev) ST(mkevent(pl, &e));
   CK(cudaEventRecord(s->ev_consumed, s->cs));
   s->ring_frames = ring_frames;
   ST(dmalloc(pl, &s->d_frames, (size_t)ring_frames * kFrameLen + (size_t)kStash * kDataLen));

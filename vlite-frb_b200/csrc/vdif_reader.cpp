@@ -4,6 +4,7 @@
 
 #include <algorithm>
 #include <cstdio>
+#include <cstring>
 
 namespace vfrb {
 
@@ -149,6 +150,41 @@ PairReader::Status PairReader::run(std::vector<int64_t>& e0, std::vector<int64_t
   }
 }
 
+size_t PairReader::run_fast(const uint8_t* fr, int64_t pay0, size_t n, std::vector<int64_t>& e0,
+                            std::vector<int64_t>& e1) {
+  if (phase_ != RUNNING || !q_.empty() || nskip_[0] || nskip_[1]) return 0;
+  const bool ts = mode_ == TS;
+  size_t k = 0;
+  for (; k + 1 < n; k += 2) {
+    uint32_t w0[2], w1[2];
+    for (int p = 0; p < 2; ++p) {
+      const uint8_t* h = fr + (k + p) * (size_t)kFrameLen;
+      std::memcpy(&w0[p], h, 4);  // seconds:30 | legacy | invalid (little-endian, vdifio.h:53-72)
+      std::memcpy(&w1[p], h + 4, 4);  // frame:24 | epoch:6 | unassigned:2
+    }
+    const int f0 = (int)(w1[0] & 0xFFFFFFu), f1 = (int)(w1[1] & 0xFFFFFFu);
+    if (f0 != expected_[0] || f1 != expected_[1]) break;  // a gap: checkframeskip decides
+    const long long s0 = w0[0] & 0x3FFFFFFFu, s1 = w0[1] & 0x3FFFFFFFu;
+    if (ts && (s0 != expsec_[0] || s1 != expsec_[1])) break;
+    // checkframeskip with no skip: advance the expected frame (and second)
+    expected_[0] = (f0 + 1) % kFramesPerSec;
+    expected_[1] = (f1 + 1) % kFramesPerSec;
+    if (ts) {
+      expsec_[0] = s0 + (expected_[0] == 0 ? 1 : 0);
+      expsec_[1] = s1 + (expected_[1] == 0 ? 1 : 0);
+    }
+    hdr_[0].frame = (uint32_t)f0;
+    hdr_[1].frame = (uint32_t)f1;
+    hdr_[0].seconds = (uint32_t)s0;
+    hdr_[1].seconds = (uint32_t)s1;
+    cur_[0] = pay0 + (int64_t)k;
+    cur_[1] = pay0 + (int64_t)k + 1;
+    e0.push_back(cur_[0]);
+    e1.push_back(cur_[1]);
+  }
+  return k;
+}
+
 }  // namespace vfrb
 
 extern "C" int vfrb_read_pairs(const uint8_t* bytes, size_t nbytes, int reader_mode, int dada_skip, size_t split,
@@ -161,13 +197,18 @@ extern "C" int vfrb_read_pairs(const uint8_t* bytes, size_t nbytes, int reader_m
   if (split == 0) split = nbytes ? nbytes : 1;
   const size_t per = std::max<size_t>(1, split / kFrameLen);
   PairReader::Status st = PairReader::STEP_NEED;
-  for (size_t k = 0; k < nfr; ++k) {
-    QFrame q;
-    vfrb_decode_header(bytes + k * kFrameLen, &q.h);
-    q.payload = (int64_t)k;
-    r.push(q);
-    if ((k + 1) % per == 0) st = r.run(a, b);
-    if (st == PairReader::STEP_ERROR) break;
+  // pieces of `per` frames, as they would arrive: fast path first, the rest
+  // queued for the general state machine
+  for (size_t k0 = 0; k0 < nfr && st != PairReader::STEP_ERROR; k0 += per) {
+    const size_t k1 = std::min(nfr, k0 + per);
+    size_t k = k0 + r.run_fast(bytes + k0 * kFrameLen, (int64_t)k0, k1 - k0, a, b);
+    for (; k < k1; ++k) {
+      QFrame q;
+      vfrb_decode_header(bytes + k * kFrameLen, &q.h);
+      q.payload = (int64_t)k;
+      r.push(q);
+    }
+    st = r.run(a, b);
   }
   if (st != PairReader::STEP_ERROR) {
     r.end_of_data();

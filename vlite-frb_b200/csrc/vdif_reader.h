@@ -51,6 +51,15 @@ class PairReader {
   // reference's return 2).
   Status run(std::vector<int64_t>& e0, std::vector<int64_t>& e1);
 
+  // Fast path of the RUNNING phase: with nothing queued and no fill frames
+  // pending, consumes in-order frame pairs straight from `frames` (nframes
+  // whole frames whose payloads are numbered pay0, pay0+1, ...) as long as
+  // each frame has the expected frame number (and second, TS), appending
+  // their pairs exactly as run() would.  Stops before the first frame that
+  // needs the general state machine; returns the frames consumed (even).
+  size_t run_fast(const uint8_t* frames, int64_t pay0, size_t nframes, std::vector<int64_t>& e0,
+                  std::vector<int64_t>& e1);
+
   bool initialised() const { return phase_ == RUNNING; }
   // header of the first pol-0 frame used (tstart for getVDIFDMJD, PIPE:525)
   const vfrb_hdr& start_header() const { return start_hdr_; }
