@@ -212,6 +212,16 @@ int vfrb_dedisperse(const vfrb_ddplan* plan, const vfrb_dd_args* a, void* stream
 size_t vfrb_dedisperse_noalloc_scratch_bytes(void);
 int vfrb_dedisperse_noalloc(const vfrb_ddplan* plan, const vfrb_dd_args* a, void* stream);
 
+/* ---- candidate search (extension: the reference's calcstats peak,
+ * PIPE:1337-1370, has no width) -------------------------------------------
+ * Per trial d of a dedispersed series dd[d][0..nt) (row stride `stride`):
+ * the best boxcar over widths 1, 2, 4, ..., max_width of
+ *   snr_w(t) = (sum_{i<w} dd[d][t+i] - w*ave[d]) / (sigma[d]*sqrt(w)),
+ * t = 0 .. nt-w, with the trial's calcstats ave/sigma (width 1 = peak).
+ * Ties: smaller width, then earlier start.  All pointers device. */
+int vfrb_boxcar(const float* dd, int ndm, int64_t nt, int64_t stride, const float* ave, const float* sigma,
+                int max_width, float* snr, int32_t* start, int32_t* width, void* stream);
+
 /* ---- K4: per-channel statistics (STATS:910-946) -------------------------
  * Per (channel, block of ncolstatblk rows): mean, variance ("sig") and the
  * outlier fraction count(x > ave + 5 sig)/npts with the reference's integer
@@ -281,6 +291,7 @@ typedef struct vfrb_params {
   float cand_snr;                  /* candidate threshold (peak SNR)         */
   int32_t device;
   int64_t device_bytes;            /* admission budget, 0 = 90% of free      */
+  int32_t boxcar_max;              /* candidates: widest boxcar (1 = peak only) */
 } vfrb_params;
 
 /* Reference defaults: 12500-point FFT, NAVE 4, NBUNDLE 32, 3908 channels,
@@ -320,6 +331,9 @@ typedef struct vfrb_result {
   const vfrb_cand* cands;
   double latency_ms;               /* data complete -> result on the host    */
   int32_t device_errors;           /* kernel error bits seen (0 = none)      */
+  const float* box_snr;            /* [ndm] best boxcar SNR, or NULL          */
+  const int32_t* box_start;        /* [ndm] its start (row0-relative)         */
+  const int32_t* box_width;        /* [ndm] its width in samples              */
 } vfrb_result;
 
 int vfrb_plan_create(vfrb_plan** plan, const vfrb_params* params);

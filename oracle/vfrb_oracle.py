@@ -403,6 +403,51 @@ def calcstats_dm(outdd: np.ndarray):
     return dict(ave=ave_f, sigma=sig_f, peak=peak.astype(np.float32), frb=frb, argmax=arg)
 
 
+# --- candidate search (new-build extension; no reference counterpart) -------
+def boxcar_best(outdd: np.ndarray, ave_f, sig_f, max_width: int):
+    """Per DM trial, the best boxcar over widths w = 1, 2, 4, ..., max_width:
+    S_w(t) = sum_{i<w} x[t+i] (FP64, t = 0 .. nt-w) and
+    snr_w(t) = (S_w(t) - w*ave) / (sigma*sqrt(w)) with the trial's calcstats
+    ave and sigma (width 1 is calcstats' peak).  Ties: the smaller width, then
+    the earlier start.  Returns (snr, start, width) arrays."""
+    x = np.asarray(outdd, np.float64)
+    ndm, nt = x.shape
+    ave = np.asarray(ave_f, np.float32).astype(np.float64)
+    sig = np.asarray(sig_f, np.float32).astype(np.float64)
+    cs = np.concatenate([np.zeros((ndm, 1)), np.cumsum(x, axis=1)], axis=1)
+    best = np.full(ndm, -np.inf)
+    bt = np.zeros(ndm, np.int64)
+    bw = np.ones(ndm, np.int64)
+    w = 1
+    while w <= max_width and w <= nt:
+        s = cs[:, w:] - cs[:, :-w]
+        snr = (s - w * ave[:, None]) / (sig[:, None] * np.sqrt(w))
+        t = snr.argmax(axis=1)
+        v = snr[np.arange(ndm), t]
+        upd = v > best
+        best[upd], bt[upd], bw[upd] = v[upd], t[upd], w
+        w *= 2
+    return best, bt, bw
+
+
+def candidates(best, start, width, dms, threshold: float, row0: int = 0):
+    """Candidates of one chunk: trials whose best boxcar SNR reaches the
+    threshold and is a local maximum over neighbouring trials (ties go to the
+    lower trial).  Returns a list of (dm_index, t, width, snr, dm)."""
+    out = []
+    n = len(best)
+    for d in range(n):
+        p = best[d]
+        if not (p >= threshold):
+            continue
+        if d > 0 and best[d - 1] > p:
+            continue
+        if d + 1 < n and best[d + 1] >= p:
+            continue
+        out.append((d, row0 + int(start[d]), int(width[d]), float(p), float(dms[d])))
+    return out
+
+
 # --- a16: calcstats per channel (STATS:910-946) -----------------------------
 def calcstats_chan(fb_bp: np.ndarray, ncolstatblk: int, nstatblks: int):
     """Per (channel, stat block of NCOLSTATBLK rows): mean, variance (named

@@ -189,3 +189,44 @@ def test_stream_fp16_form(vf):
     sa = [c["snr"] for r in f32[0] for c in r["cands"]]
     sb = [c["snr"] for r in f16[0] for c in r["cands"]]
     assert np.max(np.abs(np.array(sa) - np.array(sb)) / np.array(sa)) <= 0.01
+
+
+def test_stream_boxcar_candidates(vf, O, co):
+    """Candidates with the boxcar width search (widths 1..32): per chunk they
+    equal the oracle's rule applied to the same dedispersed series and
+    statistics; the wide pulse is found at a width > 1 near its true DM, and
+    against the FP64 oracle chain the candidate trials and SNRs agree."""
+    dms = np.arange(0, 12.0, 0.25, dtype=np.float32)
+    # chunks are 1280 rows (0.25 s): both pulses sit inside a chunk
+    buf = _vdif(1.5, seed=41, pulses=[(0.62, 5.0, 8.0, 40.0), (1.05, 9.0, 1.0, 40.0)])
+    plan, per = _stream_run(vf, dms, [buf], boxcar_max=32, cand_snr=8.0)
+    found = []
+    for r in per[0]:
+        best, start, width = O.boxcar_best(r["dd"], r["ave"], r["sigma"], 32)
+        assert np.array_equal(r["box_width"], width) and np.array_equal(r["box_start"], start)
+        assert np.allclose(r["box_snr"], best, rtol=1e-5)
+        want = O.candidates(best.astype(np.float32), start, width, dms, 8.0, r["row0"])
+        got = [(c["dm_index"], c["t"], c["width"]) for c in r["cands"]]
+        assert got == [(d, t, w) for d, t, w, _, _ in want]
+        found += r["cands"]
+    wide = [c for c in found if abs(c["dm"] - 5.0) <= 0.5]
+    assert wide and max(c["width"] for c in wide) > 1
+    assert any(abs(c["dm"] - 9.0) <= 0.5 for c in found)
+    # the full FP64 oracle chain (stream semantics) gives the same candidate trials
+    L = O.Layout(nave=2, muoslowfreq=384.0, nbundle=1)
+    rows = _oracle_rows(O, co, buf, L)
+    nbp = (rows.shape[0] // 128) * 128
+    off, _ = O.delay_table(dms, L.fch1, L.chanbw, L.tchan, L.nchanout)
+    ref = co.dedisperse_cm(co.transpose(co.bandpass(rows[:nbp])), off, nbp - int(off.max()))
+    for r in per[0]:
+        seg = ref[:, r["row0"]:r["row0"] + r["nt"]]
+        if seg.shape[1] < r["nt"]:
+            continue
+        st = O.calcstats_dm(seg)
+        best, start, width = O.boxcar_best(seg, st["ave"], st["sigma"], 32)
+        want = O.candidates(best, start, width, dms, 8.0, r["row0"])
+        # FP32 vs FP64 series: a near-tie between neighbouring trials may move a candidate by one trial
+        assert len(r["cands"]) == len(want)
+        for c, w in zip(r["cands"], want):
+            assert abs(c["dm_index"] - w[0]) <= 1
+            assert abs(c["snr"] - w[3]) <= 0.01 * w[3]

@@ -352,3 +352,28 @@ def test_transpose(vf):
     y = vf.fb_to_time_major(x)
     torch.cuda.synchronize()
     assert torch.equal(y, x.t())
+
+
+def test_boxcar_search_matches_oracle(vf, O):
+    """vfrb_boxcar: best (snr, start, width) per trial over widths 1..64,
+    against the FP64 oracle, on series with pulses of width 1 to 40 samples
+    and a padded row stride."""
+    torch = _torch()
+    rng = np.random.default_rng(17)
+    ndm, nt = 48, 1500
+    x = rng.standard_normal((ndm, nt)).astype(np.float32) * 2.0 + 0.3
+    for d, (t0, w, a) in enumerate([(100, 1, 9.0), (700, 3, 5.0), (1200, 8, 3.0), (40, 20, 2.0), (1450, 40, 1.5)]):
+        x[d * 9, t0:t0 + w] += a
+    st = O.calcstats_dm(x)
+    best, start, width = O.boxcar_best(x, st["ave"], st["sigma"], 64)
+    dev = torch.device("cuda")
+    pad = torch.zeros((ndm, nt + 37), dtype=torch.float32, device=dev)
+    pad[:, :nt] = torch.from_numpy(x).to(dev)
+    snr, s0, w0 = vf.boxcar(pad, torch.from_numpy(st["ave"]).to(dev), torch.from_numpy(st["sigma"]).to(dev), 64,
+                            nt=nt)
+    torch.cuda.synchronize()
+    assert np.array_equal(w0.cpu().numpy(), width)
+    assert np.array_equal(s0.cpu().numpy(), start)
+    assert np.allclose(snr.cpu().numpy(), best, rtol=1e-6)
+    wp = width[[0, 9, 18, 27, 36]]  # the pulse trials: best width grows with the pulse width
+    assert np.all(np.diff(wp) >= 0) and wp[0] == 1 and wp[-1] >= 16

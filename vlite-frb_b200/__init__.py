@@ -266,6 +266,23 @@ class DedispPlan:
             pass
 
 
+_lib.vfrb_boxcar.argtypes = [C.c_void_p, C.c_int, C.c_int64, C.c_int64, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p,
+                             C.c_void_p, C.c_void_p, C.c_void_p]
+
+
+def boxcar(dd, ave, sigma, max_width: int, nt=None, stream=None):
+    """Best boxcar per trial over widths 1..max_width (vfrb_boxcar): (snr, start, width) device tensors."""
+    torch = _torch()
+    ndm = dd.shape[0]
+    nt = dd.shape[1] if nt is None else nt
+    snr = torch.empty(ndm, dtype=torch.float32, device=dd.device)
+    start = torch.empty(ndm, dtype=torch.int32, device=dd.device)
+    width = torch.empty(ndm, dtype=torch.int32, device=dd.device)
+    _check(_lib.vfrb_boxcar(dd.data_ptr(), ndm, nt, dd.stride(0), ave.data_ptr(), sigma.data_ptr(), max_width,
+                            snr.data_ptr(), start.data_ptr(), width.data_ptr(), _stream(stream)), "vfrb_boxcar")
+    return snr, start, width
+
+
 def chan_stats(fb_cm, nrows: int, ncolstatblk: int, nstatblks: int, row0=0, row_mask=0xFFFFFFFF, stream=None):
     torch = _torch()
     nchan = fb_cm.shape[0]
@@ -305,7 +322,7 @@ class Params(C.Structure):
                 ("dada_skip", C.c_int32), ("storage", C.c_int32), ("q_scale", C.c_float), ("outputs", C.c_int32),
                 ("fb_block", C.c_int32), ("nstreams", C.c_int32), ("chunk_seconds", C.c_float),
                 ("ring_seconds", C.c_float), ("cand_snr", C.c_float), ("device", C.c_int32),
-                ("device_bytes", C.c_int64)]
+                ("device_bytes", C.c_int64), ("boxcar_max", C.c_int32)]
 
 
 class Cand(C.Structure):
@@ -320,7 +337,8 @@ class Result(C.Structure):
                 ("argmax", C.c_void_p), ("nchan", C.c_int32), ("fb_rows", C.c_int64), ("fb", C.c_void_p),
                 ("nstatblks", C.c_int32), ("chan_ave", C.c_void_p), ("chan_sig", C.c_void_p),
                 ("chan_outlier", C.c_void_p), ("ncand", C.c_int32), ("cands", C.c_void_p),
-                ("latency_ms", C.c_double), ("device_errors", C.c_int32)]
+                ("latency_ms", C.c_double), ("device_errors", C.c_int32), ("box_snr", C.c_void_p),
+                ("box_start", C.c_void_p), ("box_width", C.c_void_p)]
 
 
 _lib.vfrb_params_default.argtypes = [C.POINTER(Params)]
@@ -398,7 +416,8 @@ class Plan:
         ds = _arr(r.dd_sigma, ndm * nt, C.c_float)
         out["dd_sigma"] = ds.reshape(ndm, nt) if ds is not None else None
         for k, dt in (("ave", C.c_float), ("sigma", C.c_float), ("peak", C.c_float), ("frb", C.c_int32),
-                      ("argmax", C.c_int32)):
+                      ("argmax", C.c_int32), ("box_snr", C.c_float), ("box_start", C.c_int32),
+                      ("box_width", C.c_int32)):
             out[k] = _arr(getattr(r, k), ndm, dt)
         fb = _arr(r.fb, r.fb_rows * nch, C.c_float)
         out["fb"] = fb.reshape(r.fb_rows, nch) if fb is not None else None

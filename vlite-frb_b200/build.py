@@ -28,7 +28,7 @@ COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC,-Wall,-Wno-unus
           "--expt-relaxed-constexpr", "-I" + os.path.join(REPO, "include"), "-I" + CSRC]
 
 LIB_SOURCES = ["channelise.cu", "bandpass.cu", "dedisperse.cu", "vfrb_api.cpp"]
-LIB_SOURCES_OPTIONAL = ["engine.cu", "vdif_reader.cpp", "writers.cpp", "dada.cpp", "noalloc.cu"]
+LIB_SOURCES_OPTIONAL = ["engine.cu", "vdif_reader.cpp", "writers.cpp", "dada.cpp", "noalloc.cu", "candidates.cu"]
 TOOL_MAINS = ["vdifFILE2dedisp_PIPELINE.cpp", "vdifDADA2stats.cpp", "vdifDADA2timeseries.cpp", "vfrb_dada_write.cpp"]
 
 

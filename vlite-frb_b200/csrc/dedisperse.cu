@@ -229,6 +229,24 @@ __global__ void __launch_bounds__(kDdThreads) k_dedisperse(const DdKParams p) {
   if (err && p.err) atomicOr(p.err, err);
 }
 
+// calcstats from FP64 sums (PIPE:1337-1370): FP64 mean, corrected two-pass
+// variance, both stored as float; peak = max(0, (max x - ave)/sigma) in float.
+__device__ __forceinline__ void dm_finalize(int d, long long nt_out, double s, double s2, float mx, int arg,
+                                            float* ave, float* sigma, float* peak, int* frb, int* argmax) {
+  const double n = (double)nt_out;
+  const double tave = s / n;
+  const double tsig = (s2 - s * s / n) / (n - 1.0);  // == the reference's corrected two-pass form
+  const float ave_f = (float)tave;
+  const float sig_f = (float)sqrt(tsig);
+  // max_t (x - ave)/sigma in float equals f(max_t x): the map is monotone.
+  const float snr = (mx - ave_f) / sig_f;
+  if (ave) ave[d] = ave_f;
+  if (sigma) sigma[d] = sig_f;
+  if (peak) peak[d] = (snr > 0.f) ? snr : 0.f;
+  if (frb) frb[d] = (snr > 3.0f) ? 1 : 0;
+  if (argmax) argmax[d] = arg;
+}
+
 // calcstats finalize: one warp per DM reduces the time-block partials.
 __global__ void __launch_bounds__(256) k_dm_stats(const DmPartial* __restrict__ part, int ntb, int ndm,
                                                   long long nt_out, float* ave, float* sigma, float* peak,
@@ -260,18 +278,50 @@ __global__ void __launch_bounds__(256) k_dm_stats(const DmPartial* __restrict__ 
     }
   }
   if (lane != 0) return;
-  const double n = (double)nt_out;
-  const double tave = s / n;
-  const double tsig = (s2 - s * s / n) / (n - 1.0);  // == the reference's corrected two-pass form
-  const float ave_f = (float)tave;
-  const float sig_f = (float)sqrt(tsig);
-  // max_t (x - ave)/sigma in float equals f(max_t x): the map is monotone.
-  const float snr = (mx - ave_f) / sig_f;
-  if (ave) ave[d] = ave_f;
-  if (sigma) sigma[d] = sig_f;
-  if (peak) peak[d] = (snr > 0.f) ? snr : 0.f;
-  if (frb) frb[d] = (snr > 3.0f) ? 1 : 0;
-  if (argmax) argmax[d] = arg;
+  dm_finalize(d, nt_out, s, s2, mx, arg, ave, sigma, peak, frb, argmax);
+}
+
+// calcstats of whole series: one warp per DM over dd[d][0..nt) (stream mode,
+// where one dedispersion launch may cover several output chunks).
+__global__ void __launch_bounds__(256) k_series_stats(const float* __restrict__ dd, long long nt, long long stride,
+                                                      int ndm, float* ave, float* sigma, float* peak, int* frb,
+                                                      int* argmax) {
+  const int lane = threadIdx.x & 31;
+  const int d = blockIdx.x * 8 + (threadIdx.x >> 5);
+  if (d >= ndm) return;
+  const float* x = dd + (long long)d * stride;
+  double s = 0.0, s2 = 0.0;
+  float mx = -INFINITY;
+  int arg = 0x7fffffff;
+  for (long long t = lane; t < nt; t += 32) {
+    const float v = x[t];
+    s += (double)v;
+    s2 += (double)v * (double)v;
+    if (v > mx) {  // t grows: the first maximum is kept
+      mx = v;
+      arg = (int)t;
+    }
+  }
+  s = wsum(s);
+  s2 = wsum(s2);
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    const float omx = __shfl_xor_sync(0xffffffffu, mx, o);
+    const int oarg = __shfl_xor_sync(0xffffffffu, arg, o);
+    if (omx > mx || (omx == mx && oarg < arg)) {
+      mx = omx;
+      arg = oarg;
+    }
+  }
+  if (lane != 0) return;
+  dm_finalize(d, nt, s, s2, mx, arg, ave, sigma, peak, frb, argmax);
+}
+
+int launch_series_stats(const float* dd, int ndm, long long nt, long long stride, float* ave, float* sigma,
+                        float* peak, int* frb, int* argmax, cudaStream_t s) {
+  if (!dd || ndm < 1 || nt < 2 || stride < nt || nt > 0x7fffffffLL) return VFRB_ERR_ARG;
+  k_series_stats<<<(ndm + 7) / 8, 256, 0, s>>>(dd, nt, stride, ndm, ave, sigma, peak, frb, argmax);
+  return cuda_status(cudaGetLastError());
 }
 
 // Fallback for delay spreads too wide to stage: direct loads, one thread per
@@ -532,10 +582,12 @@ static int pat_launch_t(const vfrb_ddplan* pl, const RegGroup& g, const vfrb_dd_
   cudaError_t e =
       cudaFuncSetAttribute(k_dedisp_pat<T, D, TT, SMAX>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return VFRB_ERR_CUDA;
-  dim3 grid((unsigned)((a.nt_out + NT - 1) / NT), (unsigned)g.nblocks);
+  const long long ntime = (a.nt_out + NT - 1) / NT;
+  if (ntime > 65535) return VFRB_OK;  // time blocks run along grid y
+  dim3 grid((unsigned)g.nblocks, (unsigned)ntime);
   k_dedisp_pat<T, D, TT, SMAX><<<grid, kPatWarps * 32, smem, s>>>(k);
   const int st = cuda_status(cudaGetLastError());
-  if (st == VFRB_OK) *ntb = (int)grid.x;
+  if (st == VFRB_OK) *ntb = (int)grid.y;
   return st;
 }
 

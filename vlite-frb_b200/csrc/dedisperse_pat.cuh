@@ -179,8 +179,11 @@ __global__ void __launch_bounds__(kPatWarps * 32, 2) k_dedisp_pat(const DdPatPar
   const int meta_q = (3 * 2 * kPatWarps * CH + 2 * kPatWarps + 3) / 4;
   int4* tiles = smp4 + meta_q;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const long long t0 = (long long)blockIdx.x * NT;
-  const int blk = blockIdx.y;
+  // DM blocks run along x (fastest), so the CTAs working on one time window
+  // are resident together and read its filterbank rows from L2, not DRAM
+  const int blk = blockIdx.x;
+  const int tb = blockIdx.y;
+  const long long t0 = (long long)tb * NT;
   const int g = min(blk * kPatWarps + warp, p.ngroups - 1);
   const T* fb = reinterpret_cast<const T*>(p.fb);
   const int nchunks = (p.nchan + CH - 1) / CH;
@@ -312,7 +315,7 @@ __global__ void __launch_bounds__(kPatWarps * 32, 2) k_dedisp_pat(const DdPatPar
       pq.s2 = s2;
       pq.mx = mx;
       pq.arg = arg;
-      p.part[(long long)blockIdx.x * p.ndm + d] = pq;
+      p.part[(long long)tb * p.ndm + d] = pq;
     }
   }
   if (err && p.err) atomicOr(p.err, err);

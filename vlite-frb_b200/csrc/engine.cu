@@ -38,6 +38,10 @@ int ddplan_create(vfrb_ddplan** out, const int32_t* h_off, int ndm, int nchan);
 int ddplan_destroy(vfrb_ddplan* p);
 int ddplan_max_delay(const vfrb_ddplan* p);
 int ddplan_autotune(vfrb_ddplan* pl, int storage, long long nt, float* times, cudaStream_t s);
+int launch_boxcar(const float* dd, int ndm, long long nt, long long stride, const float* ave, const float* sigma,
+                  int max_width, float* snr, int* t, int* w, cudaStream_t s);
+int launch_series_stats(const float* dd, int ndm, long long nt, long long stride, float* ave, float* sigma,
+                        float* peak, int* frb, int* argmax, cudaStream_t s);
 
 static double now_ms() {
   using namespace std::chrono;
@@ -102,6 +106,8 @@ struct ResultSlot {
   vfrb_result r{};
   float *dd = nullptr, *dds = nullptr, *ave = nullptr, *sig = nullptr, *peak = nullptr, *fb = nullptr;
   int32_t *frb = nullptr, *arg = nullptr, *err = nullptr;
+  float* bsnr = nullptr;  // boxcar search: best SNR, start, width per trial
+  int32_t *bt = nullptr, *bw = nullptr;
   float *cave = nullptr, *csig = nullptr, *cout = nullptr;
   std::vector<vfrb_cand> cands;
   cudaEvent_t ev = nullptr;
@@ -174,6 +180,8 @@ struct StreamSt {
   float uscale = 1.f;  // FP16 form: the stream's single scale S
   float *d_out = nullptr, *d_sig = nullptr, *d_ave = nullptr, *d_sgm = nullptr, *d_peak = nullptr;
   int32_t *d_frb = nullptr, *d_arg = nullptr;
+  float* d_bsnr = nullptr;
+  int32_t *d_bt = nullptr, *d_bw = nullptr;
   void* d_ws = nullptr;
   size_t ws_bytes = 0;
   float *d_cave = nullptr, *d_csig = nullptr, *d_cout = nullptr, *d_fbt = nullptr;
@@ -197,6 +205,7 @@ struct vfrb_plan {
   int64_t chunk_rows = 0;
   int64_t nt_block = 0;
   int64_t launch_rows = 0;  // most rows one channelise launch produces
+  int64_t batch_chunks = 1; // stream mode: most output chunks one dedispersion launch covers
   int ncolstatblk = 0, nstatblks = 0;
   int64_t dev_bytes = 0;
   std::vector<std::unique_ptr<StreamSt>> st;
@@ -259,7 +268,7 @@ int64_t stream_bytes(const vfrb_plan* pl, int64_t ring_frames, int64_t R1, int64
   const vfrb_params& P = pl->P;
   const int64_t nch = pl->L.nchanout;
   int64_t b = ring_frames * kFrameLen + (int64_t)kStash * kDataLen + kSlotBufs * 2 * 16 * pl->launch_rows * 64;
-  const int64_t nt = P.mode == VFRB_MODE_BLOCK ? pl->nt_block : pl->chunk_rows;
+  const int64_t nt = P.mode == VFRB_MODE_BLOCK ? pl->nt_block : pl->chunk_rows * pl->batch_chunks;
   if (P.mode == VFRB_MODE_BLOCK) {
     b += (int64_t)pl->L.maxnt * nch * 4;                                    // raw block
     b += (int64_t)pl->max_delay * nch * 4;                                  // leftover
@@ -274,6 +283,11 @@ int64_t stream_bytes(const vfrb_plan* pl, int64_t ring_frames, int64_t R1, int64
     b += (int64_t)dedisperse_workspace_bytes_plan(pl->dd, nt) + 5LL * pl->ndm * 4;
   }
   return b;
+}
+
+// boxcar width search on: candidates wanted and widths beyond 1 requested
+bool boxcar_on(const vfrb_plan* pl) {
+  return (pl->P.outputs & VFRB_OUT_CANDS) && pl->P.boxcar_max > 1;
 }
 
 int alloc_slot(vfrb_plan* pl, StreamSt* s, ResultSlot** out) {
@@ -294,6 +308,11 @@ int alloc_slot(vfrb_plan* pl, StreamSt* s, ResultSlot** out) {
     ST(hmalloc(pl, &r->peak, (size_t)pl->ndm * 4));
     ST(hmalloc(pl, &r->frb, (size_t)pl->ndm * 4));
     ST(hmalloc(pl, &r->arg, (size_t)pl->ndm * 4));
+    if (boxcar_on(pl)) {
+      ST(hmalloc(pl, &r->bsnr, (size_t)pl->ndm * 4));
+      ST(hmalloc(pl, &r->bt, (size_t)pl->ndm * 4));
+      ST(hmalloc(pl, &r->bw, (size_t)pl->ndm * 4));
+    }
   }
   if (P.mode == VFRB_MODE_BLOCK && want(pl, VFRB_OUT_FB)) ST(hmalloc(pl, &r->fb, (size_t)pl->L.maxnt * nch * 4));
   if (P.mode == VFRB_MODE_BLOCK && want(pl, VFRB_OUT_CHANSTATS)) {
@@ -443,7 +462,10 @@ int run_bandpass(vfrb_plan* pl, StreamSt* s, const float* raw, int64_t in_row0, 
   return launch_bandpass(a, s->cs);
 }
 
-int run_dedisp(vfrb_plan* pl, StreamSt* s, int64_t row0, int64_t nrows_valid, int64_t nt) {
+// Dedisperse nt samples into d_out.  kernel_stats: calcstats (and the boxcar
+// search) of the whole launch, fused (block mode); otherwise each output
+// chunk gets its statistics from chunk_stats (stream mode).
+int run_dedisp(vfrb_plan* pl, StreamSt* s, int64_t row0, int64_t nrows_valid, int64_t nt, bool kernel_stats) {
   vfrb_dd_args a{};
   a.fb = s->d_cm;
   a.storage = pl->P.storage;
@@ -459,27 +481,31 @@ int run_dedisp(vfrb_plan* pl, StreamSt* s, int64_t row0, int64_t nrows_valid, in
   a.sigma_out = want(pl, VFRB_OUT_SIGMA) ? s->d_sig : nullptr;
   a.workspace = s->d_ws;
   a.workspace_bytes = s->ws_bytes;
-  const bool stats = want(pl, VFRB_OUT_DMSTATS) || want(pl, VFRB_OUT_CANDS);
+  const bool stats = kernel_stats && (want(pl, VFRB_OUT_DMSTATS) || want(pl, VFRB_OUT_CANDS));
   a.ave = stats ? s->d_ave : nullptr;
   a.sigma = stats ? s->d_sgm : nullptr;
   a.peak = stats ? s->d_peak : nullptr;
   a.frb = stats ? s->d_frb : nullptr;
   a.argmax = stats ? s->d_arg : nullptr;
   a.d_err = s->d_err;
-  return launch_dedisperse_plan(pl->dd, a, s->cs);
+  ST(launch_dedisperse_plan(pl->dd, a, s->cs));
+  if (kernel_stats && boxcar_on(pl))
+    ST(launch_boxcar(s->d_out, pl->ndm, nt, s->out_stride, s->d_ave, s->d_sgm, pl->P.boxcar_max, s->d_bsnr, s->d_bt,
+                     s->d_bw, s->cs));
+  return VFRB_OK;
 }
 
 // Copy this result's outputs to the host and queue it.
-int emit(vfrb_plan* pl, StreamSt* s, int64_t seq, int64_t row0, int64_t nt, bool with_fb) {
+int emit(vfrb_plan* pl, StreamSt* s, int64_t seq, int64_t row0, int64_t nt, bool with_fb, int64_t col0 = 0) {
   ResultSlot* r = nullptr;
   ST(alloc_slot(pl, s, &r));
   const int64_t nch = pl->L.nchanout;
   if (pl->want_dd && nt > 0) {
     if (want(pl, VFRB_OUT_DEDISP))
-      CK(cudaMemcpy2DAsync(r->dd, nt * 4, s->d_out, s->out_stride * 4, nt * 4, pl->ndm, cudaMemcpyDeviceToHost,
+      CK(cudaMemcpy2DAsync(r->dd, nt * 4, s->d_out + col0, s->out_stride * 4, nt * 4, pl->ndm, cudaMemcpyDeviceToHost,
                            s->cs));
     if (want(pl, VFRB_OUT_SIGMA))
-      CK(cudaMemcpy2DAsync(r->dds, nt * 4, s->d_sig, s->out_stride * 4, nt * 4, pl->ndm, cudaMemcpyDeviceToHost,
+      CK(cudaMemcpy2DAsync(r->dds, nt * 4, s->d_sig + col0, s->out_stride * 4, nt * 4, pl->ndm, cudaMemcpyDeviceToHost,
                            s->cs));
     if (want(pl, VFRB_OUT_DMSTATS) || want(pl, VFRB_OUT_CANDS)) {
       CK(cudaMemcpyAsync(r->ave, s->d_ave, pl->ndm * 4, cudaMemcpyDeviceToHost, s->cs));
@@ -487,6 +513,11 @@ int emit(vfrb_plan* pl, StreamSt* s, int64_t seq, int64_t row0, int64_t nt, bool
       CK(cudaMemcpyAsync(r->peak, s->d_peak, pl->ndm * 4, cudaMemcpyDeviceToHost, s->cs));
       CK(cudaMemcpyAsync(r->frb, s->d_frb, pl->ndm * 4, cudaMemcpyDeviceToHost, s->cs));
       CK(cudaMemcpyAsync(r->arg, s->d_arg, pl->ndm * 4, cudaMemcpyDeviceToHost, s->cs));
+    }
+    if (boxcar_on(pl)) {
+      CK(cudaMemcpyAsync(r->bsnr, s->d_bsnr, pl->ndm * 4, cudaMemcpyDeviceToHost, s->cs));
+      CK(cudaMemcpyAsync(r->bt, s->d_bt, pl->ndm * 4, cudaMemcpyDeviceToHost, s->cs));
+      CK(cudaMemcpyAsync(r->bw, s->d_bw, pl->ndm * 4, cudaMemcpyDeviceToHost, s->cs));
     }
   }
   if (with_fb && r->fb) CK(cudaMemcpyAsync(r->fb, s->d_fbt, (size_t)pl->L.maxnt * nch * 4, cudaMemcpyDeviceToHost, s->cs));
@@ -518,6 +549,9 @@ int emit(vfrb_plan* pl, StreamSt* s, int64_t seq, int64_t row0, int64_t nt, bool
   o.peak = stats ? r->peak : nullptr;
   o.frb = stats ? r->frb : nullptr;
   o.argmax = stats ? r->arg : nullptr;
+  o.box_snr = (stats && r->bsnr) ? r->bsnr : nullptr;
+  o.box_start = (stats && r->bt) ? r->bt : nullptr;
+  o.box_width = (stats && r->bw) ? r->bw : nullptr;
   o.nchan = (int32_t)nch;
   o.fb_rows = (with_fb && r->fb) ? pl->L.maxnt : 0;
   o.fb = (with_fb && r->fb) ? r->fb : nullptr;
@@ -553,7 +587,7 @@ int block_complete(vfrb_plan* pl, StreamSt* s) {
     c.outlier = s->d_cout;
     ST(launch_chan_stats(c, s->cs));
   }
-  if (pl->want_dd) ST(run_dedisp(pl, s, 0, L.maxnt, pl->nt_block));
+  if (pl->want_dd) ST(run_dedisp(pl, s, 0, L.maxnt, pl->nt_block, true));
   ST(emit(pl, s, s->blocks, s->blocks, pl->want_dd ? pl->nt_block : 0, with_fb));
   if (pl->want_dd && pl->max_delay > 0) {
     CK(cudaMemcpyAsync(s->d_fb_tm, s->d_left, (size_t)pl->max_delay * nch * 4, cudaMemcpyDeviceToDevice, s->cs));
@@ -565,11 +599,28 @@ int block_complete(vfrb_plan* pl, StreamSt* s) {
   return VFRB_OK;
 }
 
-int stream_chunk(vfrb_plan* pl, StreamSt* s, int64_t nt) {
-  ST(run_dedisp(pl, s, s->rows_out, s->rows_bp - s->rows_out, nt));
-  ST(emit(pl, s, s->chunks, s->rows_out, nt, false));
-  s->rows_out += nt;
-  ++s->chunks;
+// calcstats (and the boxcar search) of one output chunk held in d_out
+// columns [col0, col0 + nt): always computed per chunk from the series, so
+// the statistics do not depend on how chunks were batched.
+int chunk_stats(vfrb_plan* pl, StreamSt* s, int64_t col0, int64_t nt) {
+  if (!(want(pl, VFRB_OUT_DMSTATS) || want(pl, VFRB_OUT_CANDS))) return VFRB_OK;
+  ST(launch_series_stats(s->d_out + col0, pl->ndm, nt, s->out_stride, s->d_ave, s->d_sgm, s->d_peak, s->d_frb,
+                         s->d_arg, s->cs));
+  if (boxcar_on(pl))
+    ST(launch_boxcar(s->d_out + col0, pl->ndm, nt, s->out_stride, s->d_ave, s->d_sgm, pl->P.boxcar_max, s->d_bsnr,
+                     s->d_bt, s->d_bw, s->cs));
+  return VFRB_OK;
+}
+
+// k output chunks of nt samples each with one dedispersion launch
+int stream_chunks(vfrb_plan* pl, StreamSt* s, int64_t k, int64_t nt) {
+  ST(run_dedisp(pl, s, s->rows_out, s->rows_bp - s->rows_out, k * nt, false));
+  for (int64_t i = 0; i < k; ++i) {
+    ST(chunk_stats(pl, s, i * nt, nt));
+    ST(emit(pl, s, s->chunks, s->rows_out, nt, false, i * nt));
+    s->rows_out += nt;
+    ++s->chunks;
+  }
   return VFRB_OK;
 }
 
@@ -615,11 +666,15 @@ int process(vfrb_plan* pl, StreamSt* s, bool final_flush) {
       s->rows_bp = w1;
     }
     if (pl->want_dd)
-      while (s->rows_bp - pl->max_delay - s->rows_out >= pl->chunk_rows) ST(stream_chunk(pl, s, pl->chunk_rows));
+      for (;;) {  // a backlog of chunks is dedispersed in one launch (fills the GPU better)
+        const int64_t k = (s->rows_bp - pl->max_delay - s->rows_out) / pl->chunk_rows;
+        if (k < 1) break;
+        ST(stream_chunks(pl, s, std::min(k, pl->batch_chunks), pl->chunk_rows));
+      }
   }
   if (final_flush && pl->want_dd) {
     const int64_t rem = s->rows_bp - pl->max_delay - s->rows_out;
-    if (rem > 0) ST(stream_chunk(pl, s, rem));
+    if (rem > 0) ST(stream_chunks(pl, s, 1, rem));
   }
   return VFRB_OK;
 }
@@ -796,7 +851,7 @@ int create_stream(vfrb_plan* pl, int id, int64_t ring_frames, int64_t R1, int64_
     s->cm_mask = (unsigned)(R2 - 1);
     ST(dmalloc(pl, &s->d_cm, (size_t)nch * R2 * sb));
     CK(cudaMemsetAsync(s->d_cm, 0, (size_t)nch * R2 * sb, s->cs));
-    nt = pl->chunk_rows;
+    nt = pl->chunk_rows * pl->batch_chunks;
   }
   if (pl->want_dd) {
     s->out_stride = nt;
@@ -807,6 +862,11 @@ int create_stream(vfrb_plan* pl, int id, int64_t ring_frames, int64_t R1, int64_
     ST(dmalloc(pl, &s->d_peak, pl->ndm * 4));
     ST(dmalloc(pl, &s->d_frb, pl->ndm * 4));
     ST(dmalloc(pl, &s->d_arg, pl->ndm * 4));
+    if (boxcar_on(pl)) {
+      ST(dmalloc(pl, &s->d_bsnr, pl->ndm * 4));
+      ST(dmalloc(pl, &s->d_bt, pl->ndm * 4));
+      ST(dmalloc(pl, &s->d_bw, pl->ndm * 4));
+    }
     s->ws_bytes = dedisperse_workspace_bytes_plan(pl->dd, nt);
     ST(dmalloc(pl, &s->d_ws, s->ws_bytes));
   }
@@ -852,6 +912,7 @@ void vfrb_params_default(vfrb_params* p) {
   p->chunk_seconds = 1.f;
   p->ring_seconds = 1.f;
   p->cand_snr = 6.f;
+  p->boxcar_max = 1;
 }
 
 int vfrb_plan_create(vfrb_plan** out, const vfrb_params* prm) {
@@ -865,7 +926,8 @@ int vfrb_plan_create(vfrb_plan** out, const vfrb_params* prm) {
     return st;
   };
   if (P.nstreams < 1 || P.nstreams > 4096 || (P.mode != VFRB_MODE_BLOCK && P.mode != VFRB_MODE_STREAM) ||
-      P.storage < VFRB_F32 || P.storage > VFRB_I8 || P.ring_seconds <= 0.f || P.q_scale <= 0.f)
+      P.storage < VFRB_F32 || P.storage > VFRB_I8 || P.ring_seconds <= 0.f || P.q_scale <= 0.f ||
+      P.boxcar_max < 0 || P.boxcar_max > 65536)
     return fail(VFRB_ERR_ARG);
   if (cudaSetDevice(P.device) != cudaSuccess) return fail(VFRB_ERR_CUDA);
   int st = vfrb_layout_init(&pl->L, P.twonchan, P.nave, P.nbundle, P.muoslowfreq, P.nchanout_fixed, P.maxtime);
@@ -910,9 +972,17 @@ int vfrb_plan_create(vfrb_plan** out, const vfrb_params* prm) {
   int64_t ring_frames = std::max<int64_t>(4 * (2 * kFramesPerCal + 16), (int64_t)(P.ring_seconds * kFramesPerSec * 2));
   ring_frames += ring_frames & 1;
   pl->launch_rows = std::max<int64_t>(L.nbundle, ((ring_frames / 8) * kDataLen) / S / L.nbundle * L.nbundle);
+  if (P.mode == VFRB_MODE_STREAM) {
+    // whole rows per persistent channeliser CTA: a multiple of the SM count
+    int nsm = 148;
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, P.device);
+    if (pl->launch_rows >= nsm) pl->launch_rows = pl->launch_rows / nsm * nsm;
+    // a backlog of chunks is dedispersed in launches of about 4096 samples
+    pl->batch_chunks = std::min<int64_t>(8, std::max<int64_t>(1, (4096 + pl->chunk_rows - 1) / pl->chunk_rows));
+  }
   const int64_t R1 = (int64_t)pow2_at_least((unsigned long long)(pl->launch_rows + 512));
   const int64_t R2 = (int64_t)pow2_at_least(
-      (unsigned long long)(pl->max_delay + pl->chunk_rows + pl->launch_rows + 512));
+      (unsigned long long)(pl->max_delay + pl->chunk_rows * pl->batch_chunks + pl->launch_rows + 512));
   // admission by device memory
   const int64_t need = stream_bytes(pl, ring_frames, R1, R2) * P.nstreams;
   size_t fr = 0, tot = 0;
@@ -1011,17 +1081,20 @@ int vfrb_poll(vfrb_plan* pl, vfrb_result* out, int wait) {
   o.device_errors = *r->err;
   r->cands.clear();
   if (o.peak && o.argmax && (pl->P.outputs & VFRB_OUT_CANDS)) {
-    // candidates: per DM the chunk's peak SNR (calcstats semantics) above the
-    // threshold, kept where it is a local maximum over neighbouring trials
+    // candidates: per trial the chunk's best SNR -- the calcstats peak, or
+    // the best boxcar over widths 1 .. boxcar_max -- above the threshold,
+    // kept where it is a local maximum over neighbouring trials
+    const bool box = o.box_snr && o.box_start && o.box_width;
+    const float* best = box ? o.box_snr : o.peak;
     for (int d = 0; d < o.ndm; ++d) {
-      const float p = o.peak[d];
+      const float p = best[d];
       if (!(p >= pl->P.cand_snr)) continue;
-      if (d > 0 && o.peak[d - 1] > p) continue;
-      if (d + 1 < o.ndm && o.peak[d + 1] >= p) continue;
+      if (d > 0 && best[d - 1] > p) continue;
+      if (d + 1 < o.ndm && best[d + 1] >= p) continue;
       vfrb_cand c;
       c.dm_index = d;
-      c.width = 1;
-      c.t = o.row0 + o.argmax[d];
+      c.width = box ? o.box_width[d] : 1;
+      c.t = o.row0 + (box ? o.box_start[d] : o.argmax[d]);
       c.snr = p;
       c.dm = pl->dms[d];
       r->cands.push_back(c);
