@@ -283,9 +283,16 @@ def test_dedisperse_ring_wrap(vf, O):
     ring[:, (r0 + np.arange(rows)) & (R - 1)] = fb.T
     ref = O.dedisperse(fb.astype(np.float64), off, nt)
     plan = vf.DedispPlan(off)
-    out, _ = plan(torch.from_numpy(ring).cuda(), nt, row0=r0, row_mask=R - 1, nrows_valid=rows)
-    torch.cuda.synchronize()
-    assert np.max(np.abs(out.cpu().numpy() - ref)) <= 1e-5 * np.sqrt(np.mean(ref ** 2))
+    x = torch.from_numpy(ring).cuda()
+    # every kernel variant (those that do not apply fall back to the staged kernel);
+    # the pattern kernels copy wrapping channel rows themselves instead of in bulk
+    for v in (vf.DD_AUTO, vf.DD_STAGED, vf.DD_REG2, vf.DD_REG4, vf.DD_PAT2, vf.DD_PAT4, vf.DD_DIRECT):
+        plan.set_variant(0, v)
+        err = torch.zeros(1, dtype=torch.int32, device="cuda")
+        out, _ = plan(x, nt, row0=r0, row_mask=R - 1, nrows_valid=rows, d_err=err)
+        torch.cuda.synchronize()
+        assert int(err.item()) == 0, v
+        assert np.max(np.abs(out.cpu().numpy() - ref)) <= 1e-5 * np.sqrt(np.mean(ref ** 2)), v
 
 
 def test_dedisperse_sigma_matches_fp64(vf, O):

@@ -553,8 +553,8 @@ static int pat_launch_t(const vfrb_ddplan* pl, const RegGroup& g, const vfrb_dd_
   if (g.D != D || g.smax > SMAX || !g.d_gpat) return VFRB_OK;  // not applicable
   const int lm = (g.span + VEC - 1 + NT + SMAX + VEC - 1) / VEC * VEC;
   // two CTAs per SM: keep each under ~110 KB of shared memory
-  const int per_ch = 2 * lm * (int)sizeof(T) + 3 * 2 * kPatWarps * 4;
-  const int chunk = std::min(32, (110 * 1024 - 2 * kPatWarps * 4 - 16) / per_ch);
+  const int per_ch = 2 * lm * (int)sizeof(T) + 3 * kPatWarps * 4;
+  const int chunk = std::min(32, (110 * 1024 - kPatWarps * 4 - 32) / per_ch);
   if (chunk < 4) return VFRB_OK;
   DdPatParams k{};
   k.fb = a.fb;
@@ -577,7 +577,7 @@ static int pat_launch_t(const vfrb_ddplan* pl, const RegGroup& g, const vfrb_dd_
   k.chunk = chunk;
   k.lmax = lm;
   k.err = a.d_err;
-  const size_t meta = ((size_t)3 * 2 * kPatWarps * chunk + 2 * kPatWarps + 3) / 4 * 16;
+  const size_t meta = 16 + ((size_t)3 * kPatWarps * chunk + kPatWarps + 3) / 4 * 16;
   const size_t smem = meta + (size_t)2 * chunk * lm * sizeof(T);
   cudaError_t e =
       cudaFuncSetAttribute(k_dedisp_pat<T, D, TT, SMAX>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);

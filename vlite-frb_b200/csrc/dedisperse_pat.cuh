@@ -163,6 +163,41 @@ __device__ __forceinline__ void pat_dispatch(float (&acc)[D][TT], int pat, const
   pat_run_generic<T, D, TT, SMAX>(acc, tile, slot, pk, n, lane_off);
 }
 
+// mbarrier and bulk-copy helpers (sm_90+ PTX; no multicast)
+__device__ __forceinline__ unsigned smem_u32(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void mbar_init(unsigned long long* bar, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_fence_init() { asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory"); }
+__device__ __forceinline__ void mbar_arrive_expect_tx(unsigned long long* bar, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(bytes)
+               : "memory");
+}
+// Waits for the barrier phase with the given parity; gives up (false) after
+// a bounded number of polls instead of spinning for ever.
+__device__ __forceinline__ bool mbar_wait(unsigned long long* bar, unsigned parity) {
+  const unsigned a = smem_u32(bar);
+  for (int i = 0; i < (1 << 22); ++i) {
+    unsigned done;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(done)
+        : "r"(a), "r"(parity)
+        : "memory");
+    if (done) return true;
+  }
+  return false;
+}
+__device__ __forceinline__ void fence_proxy_async_smem() { asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory"); }
+// bytes from global to this CTA's shared memory, completing on `bar` (16-byte
+// aligned addresses, size a multiple of 16)
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, unsigned bytes, unsigned long long* bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(
+                   smem_u32(dst)),
+               "l"(src), "r"(bytes), "r"(smem_u32(bar))
+               : "memory");
+}
+
 template <typename T, int D, int TT, int SMAX>
 __global__ void __launch_bounds__(kPatWarps * 32, 2) k_dedisp_pat(const DdPatParams p) {
   constexpr int VEC = 16 / (int)sizeof(T);
@@ -171,12 +206,14 @@ __global__ void __launch_bounds__(kPatWarps * 32, 2) k_dedisp_pat(const DdPatPar
   extern __shared__ int4 smp4[];
   const int CH = p.chunk, LM = p.lmax;
   const int LMQ = LM / VEC;
-  // shared layout: slot[2][W][CH] int, pk[2][W][CH] unsigned, run[2][W][CH] int, nrun[2][W] int, tiles[2][CH][LM]
-  int* s_slot = reinterpret_cast<int*>(smp4);
-  unsigned* s_pk = reinterpret_cast<unsigned*>(s_slot + 2 * kPatWarps * CH);
-  int* s_run = reinterpret_cast<int*>(s_pk + 2 * kPatWarps * CH);
-  int* s_nrun = s_run + 2 * kPatWarps * CH;
-  const int meta_q = (3 * 2 * kPatWarps * CH + 2 * kPatWarps + 3) / 4;
+  // shared layout: full[2] mbarriers (16 B) | slot[W][CH] int | pk[W][CH] unsigned | run[W][CH] int | nrun[W] int
+  //                | tiles[2][CH][LM] (16-byte aligned)
+  unsigned long long* s_full = reinterpret_cast<unsigned long long*>(smp4);
+  int* s_slot = reinterpret_cast<int*>(smp4 + 1);
+  unsigned* s_pk = reinterpret_cast<unsigned*>(s_slot + kPatWarps * CH);
+  int* s_run = reinterpret_cast<int*>(s_pk + kPatWarps * CH);
+  int* s_nrun = s_run + kPatWarps * CH;
+  const int meta_q = 1 + (3 * kPatWarps * CH + kPatWarps + 3) / 4;
   int4* tiles = smp4 + meta_q;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   // DM blocks run along x (fastest), so the CTAs working on one time window
@@ -187,65 +224,117 @@ __global__ void __launch_bounds__(kPatWarps * 32, 2) k_dedisp_pat(const DdPatPar
   const int g = min(blk * kPatWarps + warp, p.ngroups - 1);
   const T* fb = reinterpret_cast<const T*>(p.fb);
   const int nchunks = (p.nchan + CH - 1) / CH;
+  const long long vend = p.row0 + p.nrows_valid;
+  const unsigned long long rmask = (unsigned long long)p.row_mask;
   int err = 0;
+  if (tid == 0) {
+    mbar_init(&s_full[0], 1);
+    mbar_init(&s_full[1], 1);
+    mbar_fence_init();
+  }
+  __syncthreads();
 
+  // Producer (warp 0): chunk k's rows into tile buffer b.  A channel's rows
+  // [a, a + LM) go in one bulk asynchronous copy when they are all valid (two
+  // when they wrap the ring: the split is at the ring end, a multiple of 16
+  // bytes); otherwise the warp copies them itself, with zeros outside
+  // [0, row0 + nrows_valid), before announcing the bulk bytes.
   auto stage = [&](int k, int b) {
     const int c0 = k * CH;
     const int nc = min(CH, p.nchan - c0);
-    // metadata: this warp's channels of the chunk, sorted into runs of one pattern
-    {
-      int pat = 0x10000 + lane;  // inactive lanes: a pattern of their own
-      int slot = 0;
-      unsigned pk = 0;
-      if (lane < nc) {
-        const int c = c0 + lane;
-        const long long a0 = (p.row0 + t0 + __ldg(p.bmin + (long long)blk * p.nchan + c)) & ~(long long)(VEC - 1);
-        int rel = (int)(p.row0 + t0 + __ldg(p.gbase + (long long)g * p.nchan + c) - a0);
-        if (rel < 0 || rel + NT + SMAX > LM) {  // cannot happen with a consistent plan
-          err |= kErrOffsetRange;
-          rel = 0;
-        }
-        slot = lane * LM + rel;
-        pk = __ldg(p.gpack + (long long)g * p.nchan + c);
-        pat = __ldg(p.gpat + (long long)g * p.nchan + c);
-      }
-      const unsigned same = __match_any_sync(0xffffffffu, pat);
-      const int leader = __ffs(same) - 1;
-      const bool lead = lane == leader && lane < nc;
-      const int cnt = __popc(same);
-      int incl = lead ? cnt : 0;
-#pragma unroll
-      for (int o = 1; o < 32; o <<= 1) {
-        const int y = __shfl_up_sync(0xffffffffu, incl, o);
-        if (lane >= o) incl += y;
-      }
-      const int start_l = incl - (lead ? cnt : 0);
-      const int start = __shfl_sync(0xffffffffu, start_l, leader);
-      const unsigned below = (1u << lane) - 1u;
-      const int rank = __popc(same & below);
-      const int mb = (b * kPatWarps + warp) * CH;
-      const unsigned leads = __ballot_sync(0xffffffffu, lead);
-      if (lane < nc) {
-        s_slot[mb + start + rank] = slot;
-        s_pk[mb + start + rank] = pk;
-      }
-      if (lead) s_run[mb + __popc(leads & below)] = (pat & 0xFF) | (start << 8) | (cnt << 16);
-      if (lane == 0) s_nrun[b * kPatWarps + warp] = __popc(leads);
+    long long a = 0;
+    unsigned long long ra = 0;
+    int n1 = LM;  // rows before the ring end
+    bool bulk = false;
+    if (lane < nc) {
+      a = (p.row0 + t0 + __ldg(p.bmin + (long long)blk * p.nchan + c0 + lane)) & ~(long long)(VEC - 1);
+      ra = (unsigned long long)a & rmask;
+      bulk = a >= 0 && a + LM <= vend;
+      if (ra + (unsigned long long)LM > rmask + 1ULL) n1 = (int)(rmask + 1ULL - ra);
     }
-    for (int cl = warp; cl < nc; cl += kPatWarps) {
-      const long long a = (p.row0 + t0 + __ldg(p.bmin + (long long)blk * p.nchan + c0 + cl)) & ~(long long)(VEC - 1);
+    unsigned slow = __ballot_sync(0xffffffffu, lane < nc && !bulk);
+    while (slow) {
+      const int cl = __ffs(slow) - 1;
+      slow &= slow - 1;
+      const long long ac = __shfl_sync(0xffffffffu, a, cl);
       const T* src = fb + (long long)(c0 + cl) * p.chan_stride;
       int4* dst = tiles + ((long long)b * CH + cl) * LMQ;
-      const long long vend = p.row0 + p.nrows_valid;
       for (int v = lane; v < LMQ; v += 32) {
-        const long long r = a + (long long)v * VEC;
-        int bytes = 0;
-        if (r >= 0 && r < vend) bytes = (int)(min((long long)VEC, vend - r) * (long long)sizeof(T));
-        const unsigned long long rr = (unsigned long long)(bytes ? r : 0) & (unsigned long long)p.row_mask;
-        cp_async16(dst + v, src + rr, bytes);
+        const long long r = ac + (long long)v * VEC;
+        int4 val = make_int4(0, 0, 0, 0);
+        if (r >= 0 && r + VEC <= vend) {  // a VEC-aligned group never straddles the ring end
+          val = *reinterpret_cast<const int4*>(src + ((unsigned long long)r & rmask));
+        } else if (r + VEC > 0 && r < vend) {
+          union {
+            int4 u;
+            T t[VEC];
+          } tmp;
+          tmp.u = make_int4(0, 0, 0, 0);
+#pragma unroll
+          for (int e = 0; e < VEC; ++e) {
+            const long long re = r + e;
+            if (re >= 0 && re < vend) tmp.t[e] = src[(unsigned long long)re & rmask];
+          }
+          val = tmp.u;
+        }
+        dst[v] = val;
       }
     }
-    cp_async_commit();
+    __syncwarp();
+    const unsigned nbulk = __popc(__ballot_sync(0xffffffffu, bulk));
+    fence_proxy_async_smem();  // earlier generic reads of this buffer before the async writes
+    if (lane == 0) mbar_arrive_expect_tx(&s_full[b], nbulk * (unsigned)(LM * (int)sizeof(T)));
+    __syncwarp();
+    if (bulk) {
+      int4* dst = tiles + ((long long)b * CH + lane) * LMQ;
+      const T* src = fb + (long long)(c0 + lane) * p.chan_stride;
+      bulk_g2s(dst, src + ra, (unsigned)(n1 * (int)sizeof(T)), &s_full[b]);
+      if (n1 < LM) bulk_g2s(dst + n1 / VEC, src, (unsigned)((LM - n1) * (int)sizeof(T)), &s_full[b]);
+    }
+  };
+
+  // This warp's channels of chunk k, sorted into runs of one pattern.
+  auto meta = [&](int k) {
+    const int c0 = k * CH;
+    const int nc = min(CH, p.nchan - c0);
+    int pat = 0x10000 + lane;  // inactive lanes: a pattern of their own
+    int slot = 0;
+    unsigned pk = 0;
+    if (lane < nc) {
+      const int c = c0 + lane;
+      const long long a0 = (p.row0 + t0 + __ldg(p.bmin + (long long)blk * p.nchan + c)) & ~(long long)(VEC - 1);
+      int rel = (int)(p.row0 + t0 + __ldg(p.gbase + (long long)g * p.nchan + c) - a0);
+      if (rel < 0 || rel + NT + SMAX > LM) {  // cannot happen with a consistent plan
+        err |= kErrOffsetRange;
+        rel = 0;
+      }
+      slot = lane * LM + rel;
+      pk = __ldg(p.gpack + (long long)g * p.nchan + c);
+      pat = __ldg(p.gpat + (long long)g * p.nchan + c);
+    }
+    const unsigned same = __match_any_sync(0xffffffffu, pat);
+    const int leader = __ffs(same) - 1;
+    const bool lead = lane == leader && lane < nc;
+    const int cnt = __popc(same);
+    int incl = lead ? cnt : 0;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int y = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += y;
+    }
+    const int start_l = incl - (lead ? cnt : 0);
+    const int start = __shfl_sync(0xffffffffu, start_l, leader);
+    const unsigned below = (1u << lane) - 1u;
+    const int rank = __popc(same & below);
+    const int mb = warp * CH;
+    const unsigned leads = __ballot_sync(0xffffffffu, lead);
+    if (lane < nc) {
+      s_slot[mb + start + rank] = slot;
+      s_pk[mb + start + rank] = pk;
+    }
+    if (lead) s_run[mb + __popc(leads & below)] = (pat & 0xFF) | (start << 8) | (cnt << 16);
+    if (lane == 0) s_nrun[warp] = __popc(leads);
+    __syncwarp();
   };
 
   float acc[D][TT];
@@ -254,21 +343,23 @@ __global__ void __launch_bounds__(kPatWarps * 32, 2) k_dedisp_pat(const DdPatPar
 #pragma unroll
     for (int i = 0; i < TT; ++i) acc[j][i] = 0.f;
 
-  stage(0, 0);
+  if (warp == 0) stage(0, 0);
   for (int k = 0; k < nchunks; ++k) {
-    cp_async_wait_all();
-    __syncthreads();
-    if (k + 1 < nchunks) stage(k + 1, (k + 1) & 1);
+    __syncthreads();  // every warp is done with chunk k-1: its buffer can be refilled
+    if (warp == 0 && k + 1 < nchunks) stage(k + 1, (k + 1) & 1);
+    meta(k);
+    if (!mbar_wait(&s_full[k & 1], (unsigned)(k >> 1) & 1u)) err |= kErrTimeout;
     const int b = k & 1;
     const T* tile = reinterpret_cast<const T*>(tiles + (long long)b * CH * LMQ);
-    const int mb = (b * kPatWarps + warp) * CH;
-    const int nrun = s_nrun[b * kPatWarps + warp];
+    const int mb = warp * CH;
+    const int nrun = s_nrun[warp];
 #pragma unroll 1
     for (int r = 0; r < nrun; ++r) {
       const int rd = s_run[mb + r];
       const int s0 = (rd >> 8) & 0xFF;
       pat_dispatch<T, D, TT, SMAX>(acc, rd & 0xFF, tile, s_slot + mb + s0, s_pk + mb + s0, rd >> 16, lane * TT);
     }
+    __syncwarp();  // this warp's metadata is rewritten for the next chunk
   }
 
   // epilogue: out = sum / NCHANOUT (PIPE:1534) x scale; calcstats partials per (DM, time block)

@@ -121,7 +121,8 @@ static void CUDART_CB mark_done(void* p) { static_cast<ResultSlot*>(p)->t_done =
 struct SlotBuf {
   int64_t* h = nullptr;
   int64_t* d = nullptr;
-  cudaEvent_t ev = nullptr;
+  cudaEvent_t ev = nullptr;       // upload h -> d done
+  cudaEvent_t ev_used = nullptr;  // the channeliser reading d done
 };
 
 struct StreamSt {
@@ -371,9 +372,14 @@ int launch_rows(vfrb_plan* pl, StreamSt* s, int64_t row_first, int64_t nrows, fl
     b.h[i] = entry_offset(s, s->e0[k]);
     b.h[s->slots_cap + i] = entry_offset(s, s->e1[k]);
   }
-  CK(cudaMemcpyAsync(b.d, b.h, sizeof(int64_t) * n, cudaMemcpyHostToDevice, s->cs));
-  CK(cudaMemcpyAsync(b.d + s->slots_cap, b.h + s->slots_cap, sizeof(int64_t) * n, cudaMemcpyHostToDevice, s->cs));
-  CK(cudaEventRecord(b.ev, s->cs));
+  // The upload goes on the copy stream: host-to-device copies queued on the
+  // compute stream would sit in the copy engine's queue until the compute
+  // stream reached them and hold up the frame copies behind them.  It waits
+  // for the channeliser that last read this device buffer.
+  CK(cudaStreamWaitEvent(s->xs, b.ev_used, 0));
+  CK(cudaMemcpyAsync(b.d, b.h, sizeof(int64_t) * 2 * s->slots_cap, cudaMemcpyHostToDevice, s->xs));
+  CK(cudaEventRecord(b.ev, s->xs));
+  CK(cudaStreamWaitEvent(s->cs, b.ev, 0));
   vfrb_chan_args a{};
   a.frames = s->d_frames;
   a.slots0 = b.d;
@@ -392,6 +398,7 @@ int launch_rows(vfrb_plan* pl, StreamSt* s, int64_t row_first, int64_t nrows, fl
   a.out_row_mask = mask;
   a.d_err = s->d_err;
   ST(launch_channelise(a, s->cs));
+  CK(cudaEventRecord(b.ev_used, s->cs));
   CK(cudaEventRecord(s->ev_consumed, s->cs));
   if (s->rel_n == StreamSt::kRelEv) {  // drop the oldest: later copies wait on newer (later) launches
     s->rel_head = (s->rel_head + 1) % StreamSt::kRelEv;
@@ -820,7 +827,9 @@ int create_stream(vfrb_plan* pl, int id, int64_t ring_frames, int64_t R1, int64_
     ST(hmalloc(pl, &b.h, sizeof(int64_t) * 2 * s->slots_cap));
     ST(dmalloc(pl, &b.d, sizeof(int64_t) * 2 * s->slots_cap));
     ST(mkevent(pl, &b.ev));
+    ST(mkevent(pl, &b.ev_used));
     CK(cudaEventRecord(b.ev, s->cs));
+    CK(cudaEventRecord(b.ev_used, s->cs));
   }
   ST(dmalloc(pl, &s->d_err, 4));
   CK(cudaMemsetAsync(s->d_err, 0, 4, s->cs));

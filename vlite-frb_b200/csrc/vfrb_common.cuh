@@ -20,6 +20,7 @@ constexpr int kFftN = 12500;
 constexpr int kErrSlotRange = 1;     // sample position outside the slot table
 constexpr int kErrRowRange = 2;      // FB row outside the ring
 constexpr int kErrOffsetRange = 4;   // delay outside the prepared window
+constexpr int kErrTimeout = 8;       // a bounded device wait gave up
 
 inline int cuda_status(cudaError_t e) { return e == cudaSuccess ? VFRB_OK : VFRB_ERR_CUDA; }
 
