@@ -38,31 +38,27 @@ constexpr int kNs3 = kR1 * kR2;   // 625
 
 // Twiddles, computed on the host in double precision and rounded to float:
 //   g_tw2[r-1][m] = W_625^(m r), m < 25, 1 <= r < 25   (pass 2, Ns = 25)
-//   pass 3 needs W_12500^q for q = m r < 12500 (m < 625, r < 20); with
-//   q = 125 h + l it is g_thi[h] * g_tlo[l], g_thi[h] = W_100^h (h < 100),
-//   g_tlo[l] = W_12500^l (l < 125): 1.8 kB instead of a 95 kB table.
+//   pass 3 needs W^(j r) = W_12500^(j r) for j < 625, 1 <= r < 20: with
+//   r = 5a + b it is T_a[j] * (W^j)^b, from four tables of 625 entries
+//   (T_0 = W^j, T_1 = W^5j, T_2 = W^10j, T_3 = W^15j) and at most three
+//   multiplications for (W^j)^b -- 20 kB instead of a 95 kB table, four
+//   table loads per butterfly instead of nineteen.
 // Each CTA copies the tables into shared memory once.
 constexpr int kTw2 = (kR2 - 1) * kNs2;  // 600
-constexpr int kThi = 100, kTlo = 125;
-// tlo[l] is stored at l + l/16: for r a multiple of 2..16 the half-warp's
-// indices (j r) mod 125 are spaced by r, which would put up to 16 of them in
-// one bank; the skew spreads them
-constexpr int kTloPad = kTlo + (kTlo - 1) / 16 + 1;  // 133
-__host__ __device__ constexpr int tlo_at(int l) { return l + (l >> 4); }
+constexpr int kTw3 = 4 * kM3;           // 2500
 constexpr int kAccFloats = kFftN / 2 + 2;  // 6252 >= any NCHANOUT
 constexpr int kStage = 12512;              // one pol's window bytes, padded to 16
 __device__ float2 g_tw2[kTw2];
-__device__ float2 g_thi[kThi];
-__device__ float2 g_tlo[kTloPad];
-// shared-memory layout (bytes): Z | stage[2 buffers][2 pols] | tw2 | thi | tlo | acc
+__device__ float2 g_tw3[kTw3];
+// shared-memory layout (bytes): Z | stage[2 buffers][2 pols] | tw2 | tw3 | acc
 constexpr size_t kSmZ = sizeof(float2) * kFftN;
 constexpr size_t kSmStage = (size_t)4 * kStage;
 constexpr size_t kSmTw2 = sizeof(float2) * kTw2;
-constexpr size_t kSmThi = sizeof(float2) * kThi;
-constexpr size_t kSmTlo = sizeof(float2) * ((kTloPad + 1) / 2 * 2);
-constexpr size_t kSmem = kSmZ + kSmStage + kSmTw2 + kSmThi + kSmTlo + sizeof(float) * kAccFloats;
+constexpr size_t kSmTw3 = sizeof(float2) * kTw3;
+constexpr size_t kSmem = kSmZ + kSmStage + kSmTw2 + kSmTw3 + sizeof(float) * kAccFloats;
 static_assert(kSmem <= 227 * 1024, "channeliser shared memory");
-static_assert(kSmZ % 16 == 0 && kSmStage % 16 == 0 && kStage % 16 == 0, "16-byte aligned regions");
+static_assert(kSmZ % 16 == 0 && kSmStage % 16 == 0 && kStage % 16 == 0 && kSmTw2 % 16 == 0 && kSmTw3 % 16 == 0,
+              "16-byte aligned regions");
 
 static std::mutex g_tw_mu;
 static bool g_tw_ready[64];
@@ -72,23 +68,19 @@ static int ensure_twiddles() {
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return VFRB_ERR_CUDA;
   std::lock_guard<std::mutex> lk(g_tw_mu);
   if (g_tw_ready[dev]) return VFRB_OK;
-  static float2 h2[kTw2], hh[kThi], hl[kTloPad];
+  static float2 h2[kTw2], h3[kTw3];
   for (int r = 1; r < kR2; ++r)
     for (int m = 0; m < kNs2; ++m) {
       const double a = -2.0 * M_PI * (double)((m * r) % 625) / 625.0;
       h2[(r - 1) * kNs2 + m] = make_float2((float)cos(a), (float)sin(a));
     }
-  for (int h = 0; h < kThi; ++h) {
-    const double a = -2.0 * M_PI * (double)h / 100.0;
-    hh[h] = make_float2((float)cos(a), (float)sin(a));
-  }
-  for (int l = 0; l < kTlo; ++l) {
-    const double a = -2.0 * M_PI * (double)l / (double)kFftN;
-    hl[tlo_at(l)] = make_float2((float)cos(a), (float)sin(a));
-  }
+  for (int t = 0; t < 4; ++t)
+    for (int m = 0; m < kM3; ++m) {
+      const double a = -2.0 * M_PI * (double)(((long long)(t == 0 ? 1 : 5 * t) * m) % kFftN) / (double)kFftN;
+      h3[t * kM3 + m] = make_float2((float)cos(a), (float)sin(a));
+    }
   if (cudaMemcpyToSymbol(g_tw2, h2, sizeof(h2)) != cudaSuccess) return VFRB_ERR_CUDA;
-  if (cudaMemcpyToSymbol(g_thi, hh, sizeof(hh)) != cudaSuccess) return VFRB_ERR_CUDA;
-  if (cudaMemcpyToSymbol(g_tlo, hl, sizeof(hl)) != cudaSuccess) return VFRB_ERR_CUDA;
+  if (cudaMemcpyToSymbol(g_tw3, h3, sizeof(h3)) != cudaSuccess) return VFRB_ERR_CUDA;
   g_tw_ready[dev] = true;
   return VFRB_OK;
 }
@@ -114,12 +106,16 @@ __device__ __forceinline__ void stage_window(unsigned char* __restrict__ st0, un
                                              const vfrb_chan_args& a, long long pos0, int& err) {
   const int tid = threadIdx.x;
   if (ALIGNED) {
+    // one 64-bit division per window; 32-bit arithmetic per 4-byte group
+    const long long slot0 = pos0 >= 0 ? pos0 / kDataLen : -1;
+    const int off0 = pos0 >= 0 ? (int)(pos0 - slot0 * kDataLen) : 0;
     for (int g = tid; g < kFftN / 4; g += kThreads) {
-      const long long pos = pos0 + 4LL * g;
-      const long long slot = pos / kDataLen;
-      const int off = (int)(pos - slot * kDataLen);
+      const int o = off0 + 4 * g;  // < 5000 + 12500
+      const int q = o / kDataLen;
+      const long long slot = slot0 + q;
+      const int off = o - q * kDataLen;
       long long s0 = -1, s1 = -1;
-      if (pos < 0 || slot >= a.nslots) {
+      if (slot0 < 0 || slot >= a.nslots) {
         err |= kErrSlotRange;
       } else {
         s0 = __ldg(a.slots0 + slot);
@@ -151,14 +147,13 @@ __device__ __forceinline__ void stage_window(unsigned char* __restrict__ st0, un
   }
 }
 
-// 12500-point forward FFT of the staged window into Z (natural order out).
+// Passes 1 and 2 of the 12500-point forward FFT of the staged window into Z.
 // Stockham passes: data1[(j/Ns)*Ns*R + j%Ns + r*Ns] = DFT_R(data0[j + r*N/R] * W^(r*(j%Ns)*N/(Ns*R))).
 // Pass 1 reads the staged bytes (not Z), so it needs no barrier between its
-// reads and writes; passes 2 and 3 hold their inputs in registers across
-// one barrier, so one Z buffer suffices.
-__device__ __forceinline__ void fft12500(float2* __restrict__ Z, const unsigned char* __restrict__ st0,
-                                         const unsigned char* __restrict__ st1, const float2* __restrict__ tw2,
-                                         const float2* __restrict__ thi, const float2* __restrict__ tlo) {
+// reads and writes; pass 2 holds its inputs in registers across one barrier,
+// so one Z buffer suffices.
+__device__ __forceinline__ void fft_passes12(float2* __restrict__ Z, const unsigned char* __restrict__ st0,
+                                             const unsigned char* __restrict__ st1, const float2* __restrict__ tw2) {
   const int tid = threadIdx.x;
   if (tid < kM1) {  // pass 1: R = 25, Ns = 1 (no twiddles); writes stride 25 (odd -> no bank conflicts)
     float2 v[kR1];
@@ -188,33 +183,31 @@ __device__ __forceinline__ void fft12500(float2* __restrict__ Z, const unsigned 
     }
     __syncthreads();
   }
-  {  // pass 3: R = 20, Ns = 625.  The last Stockham pass writes exactly the
-     // positions it reads (j + r*625), so butterflies are independent: no
-     // barrier between read and write, and 512 threads loop over 625.
-    for (int j = tid; j < kM3; j += kThreads) {
-      float2 u[kR3];
-#pragma unroll
-      for (int r = 0; r < kR3; ++r) u[r] = Z[j + r * kM3];
-      // twiddle W^(j r) = thi[h] * tlo[l] with j r = 125 h + l, stepped in r
-      const int h1 = j / kTlo, l1 = j - kTlo * h1;
-      int h = 0, l = 0;
-#pragma unroll
-      for (int r = 1; r < kR3; ++r) {
-        l += l1;
-        h += h1;
-        if (l >= kTlo) {
-          l -= kTlo;
-          ++h;
-        }
-        u[r] = cmul(u[r], cmul(thi[h], tlo[tlo_at(l)]));
-      }
-      dft20(u);
-#pragma unroll
-      for (int r = 0; r < kR3; ++r) Z[j + r * kNs3] = u[dft20_pos(r)];
-    }
-    __syncthreads();
-  }
 }
+
+// Pass 3 butterfly j (R = 20, Ns = 625): inputs Z[j + 625 r] times W^(j r),
+// output index r in u[dft20_pos(r)] is spectrum bin j + 625 r.
+__device__ __forceinline__ void pass3_butterfly(const float2* __restrict__ Z, const float2* __restrict__ tw3, int j,
+                                                float2 (&u)[kR3]) {
+#pragma unroll
+  for (int r = 0; r < kR3; ++r) u[r] = Z[j + r * kM3];
+  const float2 w1 = tw3[j];
+  const float2 w2 = cmul(w1, w1);
+  const float2 w3 = cmul(w2, w1);
+  const float2 w4 = cmul(w3, w1);
+  const float2 t5 = tw3[kM3 + j], t10 = tw3[2 * kM3 + j], t15 = tw3[3 * kM3 + j];
+#pragma unroll
+  for (int r = 1; r < kR3; ++r) {
+    const int a = r / 5, b = r % 5;
+    const float2 wb = b == 1 ? w1 : b == 2 ? w2 : b == 3 ? w3 : w4;
+    const float2 ta = a == 1 ? t5 : a == 2 ? t10 : t15;
+    const float2 w = a == 0 ? wb : (b == 0 ? ta : cmul(ta, wb));
+    u[r] = cmul(u[r], w);
+  }
+  dft20(u);
+}
+
+__device__ __forceinline__ float pw(float2 z) { return fmaf(z.x, z.x, z.y * z.y); }
 
 template <bool ALIGNED>
 __global__ void __launch_bounds__(kThreads, 1) k_channelise(const vfrb_chan_args a) {
@@ -223,16 +216,14 @@ __global__ void __launch_bounds__(kThreads, 1) k_channelise(const vfrb_chan_args
   float2* Z = reinterpret_cast<float2*>(sm);
   unsigned char* stage = sm + kSmZ;  // [2 buffers][2 pols][kStage]
   float2* tw2 = reinterpret_cast<float2*>(sm + kSmZ + kSmStage);
-  float2* thi = reinterpret_cast<float2*>(sm + kSmZ + kSmStage + kSmTw2);
-  float2* tlo = reinterpret_cast<float2*>(sm + kSmZ + kSmStage + kSmTw2 + kSmThi);
-  // per-bin power accumulators live in shared memory (each thread owns the
-  // same bins in every window), keeping registers for the butterflies
-  float* acc = reinterpret_cast<float*>(sm + kSmZ + kSmStage + kSmTw2 + kSmThi + kSmTlo);
+  float2* tw3 = reinterpret_cast<float2*>(sm + kSmZ + kSmStage + kSmTw2);
+  // per-bin power accumulators in shared memory; thread j owns the bins of
+  // pass-3 butterflies j and 625 - j in every window
+  float* acc = reinterpret_cast<float*>(sm + kSmZ + kSmStage + kSmTw2 + kSmTw3);
   const int tid = threadIdx.x;
   int err = 0;
   for (int i = tid; i < kTw2; i += kThreads) tw2[i] = g_tw2[i];
-  for (int i = tid; i < kThi; i += kThreads) thi[i] = g_thi[i];
-  for (int i = tid; i < kTloPad; i += kThreads) tlo[i] = g_tlo[i];
+  for (int i = tid; i < kTw3; i += kThreads) tw3[i] = g_tw3[i];
   for (int c = tid; c < a.nchanout; c += kThreads) acc[c] = 0.f;
   const float scale = 1.0f / (2.0f * (float)a.nfreq * (float)a.nave);
 
@@ -250,31 +241,56 @@ __global__ void __launch_bounds__(kThreads, 1) k_channelise(const vfrb_chan_args
     unsigned char* cur = stage + (size_t)(i & 1) * 2 * kStage;
     unsigned char* nxt = stage + (size_t)((i + 1) & 1) * 2 * kStage;
     // the buffer of window i+1 was last read by pass 1 of window i-1, which
-    // every thread has left (barriers inside fft12500)
+    // every thread has left (barriers after passes 1 and 2)
     if (i + 1 < nwin) stage_window<ALIGNED>(nxt, nxt + kStage, a, win_pos(i + 1), err);
     cp_async_commit_k1();
     cp_async_wait_1();  // this thread's copies of window i have landed
-    __syncthreads();    // ... and everybody else's
-    fft12500(Z, cur, cur + kStage, tw2, thi, tlo);
-    // epilogue: |Z_k|^2 + |Z_{N-k}|^2 for the selected bins
-    const bool last = (i % a.nave) == a.nave - 1;
-    const long long row = blockIdx.x + (i / a.nave) * gridDim.x;
-    const unsigned long long orow = (unsigned long long)(a.out_row0 + row) & (unsigned long long)a.out_row_mask;
-    float* dst = a.out + (long long)orow * a.out_row_stride;
-    for (int c = tid; c < a.nchanout; c += kThreads) {
-      const int k = a.nskip + c;
-      const float2 z1 = Z[k];
-      const float2 z2 = Z[kFftN - k];
-      const float v = acc[c] + (fmaf(z1.x, z1.x, z1.y * z1.y) + fmaf(z2.x, z2.x, z2.y * z2.y));
-      if (last) {
-        // (|X0|^2 + |X1|^2)/NFREQ averaged over NAVE spectra (PIPE:1296, 1310)
-        dst[c] = v * scale;
-        acc[c] = 0.f;
-      } else {
-        acc[c] = v;
+    __syncthreads();    // ... and everybody else's; pass 3 of window i-1 is done with Z
+    fft_passes12(Z, cur, cur + kStage, tw2);
+    // Pass 3 fused with detection.  Bins k = j + 625 r and N - k =
+    // (625 - j) + 625 (19 - r) come from butterflies j and 625 - j, so thread
+    // j computes both and adds |Z_k|^2 + |Z_{N-k}|^2 to the channel of
+    // min(k, N - k) straight from registers (j = 0 pairs with itself):
+    // pass 3 writes nothing back and there is no separate epilogue.
+    if (tid <= kM3 / 2) {
+      const int jj = tid, jp = (kM3 - jj) % kM3;
+      const bool last = (i % a.nave) == a.nave - 1;
+      const long long row = blockIdx.x + (i / a.nave) * gridDim.x;
+      const unsigned long long orow = (unsigned long long)(a.out_row0 + row) & (unsigned long long)a.out_row_mask;
+      float* dst = a.out + (long long)orow * a.out_row_stride;
+      float mag[kR3];
+      float2 u[kR3];
+      if (jj != 0) {
+        pass3_butterfly(Z, tw3, jp, u);
+#pragma unroll
+        for (int r = 0; r < kR3; ++r) mag[r] = pw(u[dft20_pos(r)]);
+      }
+      pass3_butterfly(Z, tw3, jj, u);
+#pragma unroll
+      for (int r = 0; r < kR3; ++r) {
+        float p;
+        int bin;
+        if (jj == 0) {  // bins 625 r and 625 (20 - r); r = 10 is the Nyquist bin (counted twice, as N - k = k)
+          if (r == 0 || r > kR3 / 2) continue;
+          p = pw(u[dft20_pos(r)]) + pw(u[dft20_pos(kR3 - r)]);
+          bin = kM3 * r;
+        } else {
+          p = pw(u[dft20_pos(r)]) + mag[kR3 - 1 - r];
+          bin = r < kR3 / 2 ? jj + kM3 * r : jp + kM3 * (kR3 - 1 - r);
+        }
+        const int c = bin - a.nskip;
+        if (c >= 0 && c < a.nchanout) {
+          const float v = acc[c] + p;
+          if (last) {
+            // (|X0|^2 + |X1|^2)/NFREQ averaged over NAVE spectra (PIPE:1296, 1310)
+            dst[c] = v * scale;
+            acc[c] = 0.f;
+          } else {
+            acc[c] = v;
+          }
+        }
       }
     }
-    __syncthreads();  // Z is rewritten by the next window's pass 1
   }
   if (err && a.d_err) atomicOr(a.d_err, err);
 }
