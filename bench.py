@@ -545,6 +545,9 @@ def main():
         except Exception as e:  # noqa: BLE001
             line["gpu_reference"] = {"error": str(e)[:200]}
     line["e2e_candidates"] = len(e2e["cands"])
+    # the same candidates clustered across trials and chunks (vfrb_cluster_cands:
+    # within 16 trials and 50 samples), i.e. one entry per detected pulse
+    line["e2e_clusters"] = len(vf.cluster_cands(e2e["cands"], dm_tol=16, t_tol=50)[0])
     print(dumps(line))
     if dist:
         import torch.distributed as d

@@ -130,8 +130,31 @@ typedef struct vfrb_bp_args {
   float* tm_out;             /* device time-major F32 copy of the result, or NULL */
   int64_t tm_row_stride;
   int32_t* d_err;
+  int32_t subtract_mode;     /* 0: cal windows (subtractbpCAL); 1: copy only,
+                              * no subtraction (feeds vfrb_subtract_bp_full)  */
 } vfrb_bp_args;
 int vfrb_bandpass(const vfrb_bp_args* a, void* stream);
+
+/* ---- Optional RFI modes the reference keeps as dead code ----------------
+ * Both work in place on a channel-major FP32 filterbank
+ * fb_cm[c * chan_stride + ((row0 + t) & row_mask)], t < nrows; row_mask
+ * 0xffffffff means a linear run (row0 + nrows <= chan_stride), otherwise a
+ * power-of-two ring of row_mask + 1 <= chan_stride rows.  nchan, nrows >= 2.
+ *
+ * vfrb_subtract_bp_full replaces subtractbp (PIPE:1372-1424; its call is
+ * commented out at PIPE:712): per channel, one clipped mean over the whole
+ * block is subtracted.  The reference's arithmetic is kept: the first mean
+ * divides the channel sum by NCHANOUT (nchan), not by the row count; the
+ * clip is the open interval ave +- 3*sig with sig the variance about that
+ * value; an empty clip gives NaN.
+ *
+ * vfrb_subtract_zero replaces subtractZERO (PIPE:1478-1515; commented out at
+ * PIPE:661, after subtractbpCAL): per row, the clipped mean across channels
+ * (count floored at 1) is subtracted from every channel (zero-DM removal). */
+int vfrb_subtract_bp_full(float* fb_cm, int64_t chan_stride, int64_t row0, uint32_t row_mask, int nchan,
+                          int64_t nrows, void* stream);
+int vfrb_subtract_zero(float* fb_cm, int64_t chan_stride, int64_t row0, uint32_t row_mask, int nchan,
+                       int64_t nrows, void* stream);
 
 /* ---- K3: dedispersion + per-DM statistics ------------------------------
  * Replaces dedisp_execute (PIPE:671, dedisp library, semantics unpinned)
@@ -292,7 +315,15 @@ typedef struct vfrb_params {
   int32_t device;
   int64_t device_bytes;            /* admission budget, 0 = 90% of free      */
   int32_t boxcar_max;              /* candidates: widest boxcar (1 = peak only) */
+  int32_t bp_mode;                 /* VFRB_BP_CAL (subtractbpCAL) or VFRB_BP_FULL
+                                    * (subtractbp, PIPE:1372); FULL: block
+                                    * mode, FP32 storage only                 */
+  int32_t zero_dm;                 /* 1: subtractZERO after the bandpass
+                                    * (PIPE:1478); block mode, FP32 only      */
 } vfrb_params;
+
+#define VFRB_BP_CAL 0
+#define VFRB_BP_FULL 1
 
 /* Reference defaults: 12500-point FFT, NAVE 4, NBUNDLE 32, 3908 channels,
  * MAXTIME 70 s, block mode, FP32, one stream. */
@@ -306,10 +337,24 @@ typedef struct vfrb_cand {
   float dm;
 } vfrb_cand;
 
+/* Friends-of-friends clustering of candidates across trials and time (no
+ * reference counterpart).  Friends: |dm_index_a - dm_index_b| <= dm_tol and
+ * max(t_a, t_b) - min(t_a + width_a, t_b + width_b) <= t_tol.  Writes one
+ * entry per connected component to out[] (capacity n): its brightest member
+ * (ties: lower dm_index, then earlier t), ordered by t then dm_index; *nout =
+ * their count; cluster_of[i] (optional, n entries) = the cluster of in[i].
+ * Candidates from several results can be concatenated and clustered together. */
+int vfrb_cluster_cands(const vfrb_cand* in, int32_t n, int32_t dm_tol, int64_t t_tol, vfrb_cand* out,
+                       int32_t* nout, int32_t* cluster_of);
+
 typedef struct vfrb_result {
   int32_t stream;
   int64_t seq;                     /* block (block mode) or chunk index      */
-  int64_t row0;                    /* absolute FB row of output sample 0     */
+  int64_t row0;                    /* absolute FB row of output sample 0 (block
+                                    * mode: of block row 0; block rows from
+                                    * (max_delay/NBUNDLE)*NBUNDLE on lie
+                                    * max_delay mod NBUNDLE rows later, as the
+                                    * reference's carry overwrites them)    */
   double tstart_mjd;               /* getVDIFDMJD of the first frame used    */
   int32_t ndm;
   int64_t nt;

@@ -55,6 +55,10 @@ __global__ void sumpower(cufftComplex* freqout0, cufftComplex* freqout1, cufftRe
 __global__ void avepower(cufftReal* powTOT, cufftReal* powAVE);
 __global__ void convertarray(cufftReal* time, unsigned char* utime);
 __global__ void subtractbpCAL(cufftReal* FULLFB);
+#if defined(REF_PIPE) || defined(REF_TS)
+__global__ void subtractbp(cufftReal* FULLFB);
+__global__ void subtractZERO(cufftReal* FULLFB);
+#endif
 #if defined(REF_PIPE)
 typedef float dedisp_float_t;
 extern __constant__ int CNTIME_OUTDD, CNDM;
@@ -340,6 +344,38 @@ extern "C" int ref_gpu_chanstats(const float* h_fb, int maxnt, int nchanout, int
   CKR(cudaMemcpy(csig, s, sb, cudaMemcpyDeviceToHost));
   CKR(cudaMemcpy(cout, o, sb, cudaMemcpyDeviceToHost));
   cudaFree(fb); cudaFree(a); cudaFree(s); cudaFree(o);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  return 0;
+}
+#endif
+
+#if defined(REF_PIPE) || defined(REF_TS)
+// ---- GPU: the dead-code modes subtractbp (kind 0) / subtractZERO (kind 1)
+// in place on a [maxnt][nchanout] block.  Both kernels give each thread one
+// independent channel (subtractbp) or row (subtractZERO), so any grid that
+// covers them computes what the reference's launch would.
+extern "C" int ref_gpu_subtract_mode(float* h_fb, int maxnt, int nchanout, int kind, float* ms) {
+  CKR(cudaMemcpyToSymbol(CNCHANOUT, &nchanout, sizeof(int)));
+  CKR(cudaMemcpyToSymbol(CMAXNT, &maxnt, sizeof(int)));
+  float* fb;
+  const size_t bytes = sizeof(float) * (size_t)maxnt * nchanout;
+  CKR(cudaMalloc(&fb, bytes));
+  CKR(cudaMemcpy(fb, h_fb, bytes, cudaMemcpyHostToDevice));
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  cudaEventRecord(e0, 0);
+  if (kind == 0)
+    subtractbp<<<(nchanout + 127) / 128, 128>>>(fb);
+  else
+    subtractZERO<<<(maxnt + 127) / 128, 128>>>(fb);
+  cudaEventRecord(e1, 0);
+  CKR(cudaEventSynchronize(e1));
+  CKR(cudaGetLastError());
+  cudaEventElapsedTime(ms, e0, e1);
+  CKR(cudaMemcpy(h_fb, fb, bytes, cudaMemcpyDeviceToHost));
+  cudaFree(fb);
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   return 0;

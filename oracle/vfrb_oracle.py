@@ -403,6 +403,41 @@ def calcstats_dm(outdd: np.ndarray):
     return dict(ave=ave_f, sigma=sig_f, peak=peak.astype(np.float32), frb=frb, argmax=arg)
 
 
+# --- dead-code bandpass modes (options; PIPE:1372-1424, 1478-1515) ----------
+def subtract_bp_full(fb: np.ndarray) -> np.ndarray:
+    """subtractbp (PIPE:1372-1424), one clipped mean per channel over the whole
+    block, fb[MAXNT][NCHANOUT] time-major.  As in the reference, the first
+    mean divides the sum by NCHANOUT (not by the number of rows), "sig" is the
+    corrected two-pass variance about that value, the clip is the open
+    interval ave +- 3 sig, and an empty clip window divides by zero (NaN)."""
+    x = np.asarray(fb, np.float64)
+    n, nch = x.shape
+    ave = x.sum(axis=0) / nch
+    d = x - ave
+    sig = ((d * d).sum(axis=0) - d.sum(axis=0) ** 2 / n) / (n - 1)
+    hi, lo = ave + 3.0 * sig, ave - 3.0 * sig
+    keep = (x < hi) & (x > lo)
+    with np.errstate(invalid="ignore", divide="ignore"):
+        cm = (x * keep).sum(axis=0) / keep.sum(axis=0)
+    return x - cm
+
+
+def subtract_zero(fb: np.ndarray) -> np.ndarray:
+    """subtractZERO (PIPE:1478-1515): per time row, the clipped mean over the
+    channels (mean, corrected variance "sig", open interval ave +- 3 sig,
+    count floored at 1) is subtracted from every channel (zero-DM removal)."""
+    x = np.asarray(fb, np.float64)
+    n, nch = x.shape
+    ave = x.sum(axis=1) / nch
+    d = x - ave[:, None]
+    sig = ((d * d).sum(axis=1) - d.sum(axis=1) ** 2 / nch) / (nch - 1)
+    hi, lo = ave + 3.0 * sig, ave - 3.0 * sig
+    keep = (x < hi[:, None]) & (x > lo[:, None])
+    cnt = np.maximum(keep.sum(axis=1), 1)
+    cm = (x * keep).sum(axis=1) / cnt
+    return x - cm[:, None]
+
+
 # --- candidate search (new-build extension; no reference counterpart) -------
 def boxcar_best(outdd: np.ndarray, ave_f, sig_f, max_width: int):
     """Per DM trial, the best boxcar over widths w = 1, 2, 4, ..., max_width:
@@ -446,6 +481,42 @@ def candidates(best, start, width, dms, threshold: float, row0: int = 0):
             continue
         out.append((d, row0 + int(start[d]), int(width[d]), float(p), float(dms[d])))
     return out
+
+
+def cluster_cands(cands, dm_tol: int, t_tol: int):
+    """Friends-of-friends clustering (new-build extension): candidates
+    (dm_index, t, width, snr) are friends when |dm_a - dm_b| <= dm_tol and
+    max(t_a, t_b) - min(t_a + w_a, t_b + w_b) <= t_tol; clusters are the
+    connected components, each reported by its brightest member (ties: lower
+    dm_index, then earlier t), ordered by (t, dm_index).  O(n^2) pairs, for
+    small lists.  Returns (representatives, labels)."""
+    n = len(cands)
+    parent = list(range(n))
+
+    def find(a):
+        while parent[a] != a:
+            a = parent[a]
+        return a
+
+    for i in range(n):
+        for j in range(i + 1, n):
+            a, b = cands[i], cands[j]
+            gap = max(a[1], b[1]) - min(a[1] + a[2], b[1] + b[2])
+            if abs(a[0] - b[0]) <= dm_tol and gap <= t_tol:
+                ri, rj = find(i), find(j)
+                if ri != rj:
+                    parent[max(ri, rj)] = min(ri, rj)
+    groups = {}
+    for i in range(n):
+        groups.setdefault(find(i), []).append(i)
+    reps = []
+    for root, mem in groups.items():
+        best = min(mem, key=lambda k: (-cands[k][3], cands[k][0], cands[k][1]))
+        reps.append((root, best))
+    reps.sort(key=lambda rb: (cands[rb[1]][1], cands[rb[1]][0]))
+    label_of_root = {root: k for k, (root, _) in enumerate(reps)}
+    labels = [label_of_root[find(i)] for i in range(n)]
+    return [cands[b] for _, b in reps], labels
 
 
 # --- a16: calcstats per channel (STATS:910-946) -----------------------------

@@ -58,6 +58,7 @@ def test_block_mode_pipe_chain(vf, O, co):
     rows = _oracle_rows(O, co, buf, L)
     blocks = list(O.run_blocks(rows, L, md))
     assert len(res) == len(blocks) == 2
+    assert [r["row0"] for r in res] == [0, L.maxnt - md]  # absolute row of each block's row 0
     for r, (q, fb) in zip(res, blocks):
         bp = co.bandpass(fb)
         dd = co.dedisperse_cm(co.transpose(bp), off, L.maxnt - md)
@@ -71,6 +72,38 @@ def test_block_mode_pipe_chain(vf, O, co):
             _close(r["fb"], bp, 5e-5, "block 1 bandpassed FB")
         else:
             assert r["fb"] is None
+
+
+def test_block_mode_rfi_modes(vf, O, co):
+    """The reference's dead-code options as plan parameters: whole-block
+    subtractbp (PIPE:1372) in place of subtractbpCAL, then subtractZERO
+    (PIPE:1478), before dedispersion and calcstats."""
+    nave, maxtime = 2, 0.8
+    dms = np.arange(0, 10.5, 0.5, dtype=np.float32)
+    buf = _vdif(1.2, seed=12, pulses=[(0.5, 6.0, 2.0, 40.0)])
+    plan = vf.Plan(dms, nave=nave, muoslowfreq=384.0, maxtime=maxtime, mode=vf.MODE_BLOCK,
+                   outputs=vf.OUT_DEDISP | vf.OUT_DMSTATS | vf.OUT_FB, bp_mode=vf.BP_FULL, zero_dm=1)
+    plan.push(0, buf)
+    plan.push(0, None)
+    res = plan.drain()
+    L = O.Layout(nave=nave, muoslowfreq=384.0, maxtime=maxtime)
+    off, md = O.delay_table(dms, L.fch1, L.chanbw, L.tchan, L.nchanout)
+    rows = _oracle_rows(O, co, buf, L)
+    blocks = list(O.run_blocks(rows, L, md))
+    assert len(res) == len(blocks) >= 1
+    for r, (q, fb) in zip(res, blocks):
+        x = O.subtract_zero(O.subtract_bp_full(fb))
+        assert not np.isnan(x).any()
+        _close(r["fb"], x, 5e-5, f"block {q} whole-block BP + zero-DM FB")
+        dd = co.dedisperse_cm(co.transpose(x), off, L.maxnt - md)
+        _close(r["dd"], dd, 5e-5, f"block {q} dedispersed")
+        st = O.calcstats_dm(dd)
+        # zero-DM removal leaves the DM-0 series at rounding level (its sigma
+        # ~1e-14 in FP64, ~1e-6 in FP32): statistics of such trials are noise
+        ok = st["sigma"] > 1e-6 * st["sigma"].max()
+        assert not ok[0] and ok[1:].all()
+        assert np.array_equal(r["frb"][ok], st["frb"][ok])
+        assert np.allclose(r["sigma"][ok], st["sigma"][ok], rtol=1e-4)
 
 
 def test_block_mode_ts_chain(vf, O, co):
@@ -110,6 +143,7 @@ def test_block_mode_stats_chain(vf, O, co):
     nblk = int(np.float32(maxtime) / np.float32(tstat))
     blocks = list(O.run_stats_blocks(rows, L))
     assert len(res) == len(blocks) == 2
+    assert [r["row0"] for r in res] == [0, L.maxnt]  # no overlap: blocks follow each other
     for r, (q, fb) in zip(res, blocks):
         bp = co.bandpass(fb)
         a, s, o = O.calcstats_chan(bp, ncol, nblk)

@@ -115,3 +115,52 @@ def test_presto_inf_matches_oracle(vf, O):
     want = O.presto_inf(args[0].decode(), *args[1:])
     assert buf.value.decode() == want
     assert lib.vfrb_presto_inf(None, 0, None, *args[1:]) == -1
+
+
+@pytest.mark.parametrize("kw,status", [
+    (dict(bp_mode=2), 4),                                      # unknown bandpass mode: VFRB_ERR_ARG
+    (dict(zero_dm=3), 4),
+    (dict(bp_mode=1, mode=1), 5),                              # whole-block modes: block mode only
+    (dict(zero_dm=1, mode=1), 5),
+    (dict(bp_mode=1, storage=1), 5),                           # ... and FP32 storage only
+    (dict(zero_dm=1, storage=2), 5),
+])
+def test_plan_rejects_unsupported_rfi_modes(vf, kw, status):
+    """Parameter checks run before any CUDA call, so they need no GPU."""
+    with pytest.raises(vf.VfrbError) as e:
+        vf.Plan(np.array([0.0, 10.0], np.float32), **kw)
+    assert e.value.status == status
+
+
+def test_cluster_cands_known_answer(vf):
+    c = [dict(dm_index=10, t=1000, width=4, snr=9.0), dict(dm_index=11, t=1002, width=1, snr=12.0),
+         dict(dm_index=13, t=1001, width=2, snr=7.0),   # within 2 trials of 11: joins through it
+         dict(dm_index=30, t=1000, width=1, snr=8.0),   # far in DM: its own cluster
+         dict(dm_index=10, t=1010, width=1, snr=6.5),   # 6 samples after 1000+4: apart for t_tol 5
+         dict(dm_index=12, t=900, width=1, snr=6.0)]
+    cl, lab = vf.cluster_cands(c, dm_tol=2, t_tol=5)
+    assert [(x["dm_index"], x["t"], x["snr"]) for x in cl] == [(12, 900, 6.0), (30, 1000, 8.0), (11, 1002, 12.0),
+                                                             (10, 1010, 6.5)]
+    assert list(lab) == [2, 2, 2, 1, 3, 0]
+    cl, lab = vf.cluster_cands(c, dm_tol=2, t_tol=6)  # gap 1010 - 1004 = 6: now friends
+    assert len(cl) == 3 and lab[4] == lab[0]
+    cl, lab = vf.cluster_cands([], 2, 5)
+    assert cl == [] and len(lab) == 0
+    with pytest.raises(vf.VfrbError):
+        vf.cluster_cands(c, dm_tol=-1)
+    with pytest.raises(vf.VfrbError):
+        vf.cluster_cands([dict(dm_index=0, t=0, width=0, snr=7.0)])
+
+
+@pytest.mark.parametrize("seed", [0, 1, 2])
+def test_cluster_cands_matches_oracle(vf, O, seed):
+    rng = np.random.default_rng(seed)
+    n = 300
+    c = [dict(dm_index=int(rng.integers(0, 60)), t=int(rng.integers(0, 4000)), width=int(2 ** rng.integers(0, 5)),
+              snr=float(np.float32(rng.integers(60, 90) / 8.0))) for _ in range(n)]  # repeated SNRs: tie rules
+    for dm_tol, t_tol in ((0, 0), (2, 8), (5, 40)):
+        cl, lab = vf.cluster_cands(c, dm_tol=dm_tol, t_tol=t_tol)
+        tup = [(x["dm_index"], x["t"], x["width"], x["snr"]) for x in c]
+        ocl, olab = O.cluster_cands(tup, dm_tol, t_tol)
+        assert [(x["dm_index"], x["t"], x["width"], x["snr"]) for x in cl] == ocl
+        assert list(lab) == olab

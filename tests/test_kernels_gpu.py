@@ -10,7 +10,9 @@ Tolerances (stated here, used below):
   * dedispersed series (FP32): max |gpu - oracle| <= 1e-5 * rms(oracle series);
   * per-DM ave/sigma: relative <= 1e-5; peak: relative <= 1e-4; FRB flag exact;
   * FP16 storage: <= 3e-3 * rms, int8 (q=16) storage: <= 0.12 * rms (errors reported);
-  * per-channel stats: relative <= 1e-6, outlier fraction exact.
+  * per-channel stats: relative <= 1e-6, outlier fraction exact;
+  * subtractbp / subtractZERO modes: <= 1e-6 * max|input|, NaN where the
+    oracle is NaN.
 """
 import numpy as np
 import pytest
@@ -165,6 +167,89 @@ def test_bandpass_ring_in_and_out(vf, O):
     torch.cuda.synchronize()
     got = ring_out.cpu().numpy()[:, (900 + np.arange(rows)) & 1023].T
     assert np.max(np.abs(got - ref)) <= 1e-6 * np.abs(x).max()
+
+
+def _rfi_fb(rows, nch, seed):
+    """Bandpassed-like data (zero mean, per-channel sd 1-3) with RFI: spikes,
+    a broadband row, a constant channel (empty subtractbp clip) and a channel
+    with a wide clip window."""
+    rng = np.random.default_rng(seed)
+    x = rng.standard_normal((rows, nch)) * rng.uniform(1, 3, nch)
+    x[rng.integers(0, rows, 40), rng.integers(0, nch, 40)] += 60.0
+    x[rows // 3, :] += 25.0
+    x[:, 5] = 2.0
+    x[:, 9] = x[:, 9] * 40 + 100.0
+    return x.astype(np.float32)
+
+
+@pytest.mark.parametrize("rows,nch", [(700, 96), (129, 300)])
+def test_subtract_modes_match_oracle(vf, O, rows, nch):
+    """subtractbp (whole block) and subtractZERO in place on the channel-major
+    FB: FP64 sums, so within one float rounding of the FP64 oracle, NaN where
+    the reference's empty clip divides by zero."""
+    torch = _torch()
+    x = _rfi_fb(rows, nch, seed=rows)
+    tol = 1e-6 * np.abs(x).max()
+    dev = torch.device("cuda")
+    cm = torch.from_numpy(np.ascontiguousarray(x.T)).to(dev)
+    vf.subtract_bp_full(cm)
+    ref = O.subtract_bp_full(x.astype(np.float64))
+    got = cm.cpu().numpy().T.astype(np.float64)
+    assert np.array_equal(np.isnan(got), np.isnan(ref)) and np.isnan(ref[:, 5]).all()
+    ok = ~np.isnan(ref)
+    assert np.max(np.abs(got[ok] - ref[ok])) <= tol
+    cm = torch.from_numpy(np.ascontiguousarray(x.T)).to(dev)
+    vf.subtract_zero(cm)
+    torch.cuda.synchronize()
+    ref = O.subtract_zero(x.astype(np.float64))
+    assert np.max(np.abs(cm.cpu().numpy().T - ref)) <= tol
+
+
+def test_subtract_modes_ring_and_args(vf, O):
+    torch = _torch()
+    rows, nch = 300, 50
+    x = _rfi_fb(rows, nch, seed=4)
+    dev = torch.device("cuda")
+    ring = torch.full((nch, 512), 7.0, device=dev)
+    idx = torch.from_numpy((450 + np.arange(rows)) & 511).to(dev)
+    for fn, orc in ((vf.subtract_bp_full, O.subtract_bp_full), (vf.subtract_zero, O.subtract_zero)):
+        ring[:, idx] = torch.from_numpy(np.ascontiguousarray(x.T)).to(dev)
+        fn(ring, nrows=rows, row0=450, row_mask=511)
+        torch.cuda.synchronize()
+        got = ring.cpu().numpy()
+        ref = orc(x.astype(np.float64))
+        g = got[:, (450 + np.arange(rows)) & 511].T
+        ok = ~np.isnan(ref)
+        assert np.array_equal(np.isnan(g), ~ok)
+        assert np.max(np.abs(g[ok] - ref[ok])) <= 1e-6 * np.abs(x).max()
+        untouched = np.ones(512, bool)
+        untouched[(450 + np.arange(rows)) & 511] = False
+        assert (got[:, untouched] == 7.0).all()
+    # rows outside the buffer, a ring that is not a power of two or longer than
+    # the channel stride, too few channels or rows: VFRB_ERR_ARG, nothing launched
+    bad = [dict(nrows=rows, row0=300), dict(nrows=rows, row_mask=299), dict(nrows=rows, row_mask=1023),
+           dict(nrows=600, row_mask=511), dict(nrows=1)]
+    for kw in bad:
+        with pytest.raises(RuntimeError):
+            vf.subtract_zero(ring, **kw)
+        with pytest.raises(RuntimeError):
+            vf.subtract_bp_full(ring, **kw)
+    with pytest.raises(RuntimeError):
+        vf.subtract_zero(ring[:1])
+
+
+def test_bandpass_copy_mode(vf):
+    """subtract_mode 1: the rows are transposed to channel-major unchanged."""
+    torch = _torch()
+    x = _rand_fb(300, 70, seed=6)
+    dev = torch.device("cuda")
+    wm = torch.full((3, 70), 5.0, device=dev)
+    out = vf.bandpass(torch.from_numpy(x).to(dev), subtract_mode=1, win_mean=wm)
+    torch.cuda.synchronize()
+    assert np.array_equal(out.cpu().numpy(), x.T)
+    assert (wm.cpu().numpy() == 0).all()
+    with pytest.raises(RuntimeError):
+        vf.bandpass(torch.from_numpy(x).to(dev), subtract_mode=2)
 
 
 def _dd_case(ndm=40, nch=256, nt=1000, seed=2, dm_max=30.0, irregular=False):

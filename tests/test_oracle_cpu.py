@@ -43,3 +43,67 @@ def test_c_chain_matches_numpy(co, O):
     cs_n = O.calcstats_chan(bp_n, 200, 3)
     for x, y in zip(cs_c, cs_n):
         assert np.allclose(x, y, rtol=1e-6, atol=1e-9)
+
+
+def _loop_subtract_bp_full(fb):
+    """Statement-by-statement transcription of subtractbp (PIPE:1372-1424) in
+    FP64 loops, checking the vectorised oracle on a small case."""
+    x = np.array(fb, np.float64)
+    nt, nch = x.shape
+    for c in range(nch):
+        ave = sum(x[j, c] for j in range(nt)) / nch  # PIPE:1380, divides by CNCHANOUT
+        s = s2 = 0.0
+        for j in range(nt):
+            s2 += (x[j, c] - ave) ** 2
+            s += x[j, c] - ave
+        sig = (s2 - s * s / nt) / (nt - 1)
+        hi, lo = ave + 3.0 * sig, ave - 3.0 * sig
+        a, i = 0.0, 0
+        for j in range(nt):
+            if lo < x[j, c] < hi:
+                a += x[j, c]
+                i += 1
+        m = a / i if i else float("nan")
+        x[:, c] -= m
+    return x
+
+
+def _loop_subtract_zero(fb):
+    """Transcription of subtractZERO (PIPE:1478-1515) in FP64 loops."""
+    x = np.array(fb, np.float64)
+    nt, nch = x.shape
+    for t in range(nt):
+        ave = sum(x[t]) / nch
+        s = s2 = 0.0
+        for j in range(nch):
+            s2 += (x[t, j] - ave) ** 2
+            s += x[t, j] - ave
+        sig = (s2 - s * s / nch) / (nch - 1)
+        hi, lo = ave + 3.0 * sig, ave - 3.0 * sig
+        a, i = 0.0, 0
+        for j in range(nch):
+            if lo < x[t, j] < hi:
+                a += x[t, j]
+                i += 1
+        x[t] -= a / max(i, 1)
+    return x
+
+
+def test_rfi_modes_oracle_matches_loops(O):
+    rng = np.random.default_rng(5)
+    nt, nch = 60, 9
+    fb = rng.standard_normal((nt, nch)) * 0.2
+    fb[:, 2] = fb[:, 2] * 50 + 40.0  # variance 100: the window about sum/nch = 267 keeps every row
+    fb[:, 3] += 40.0        # variance 0.04 about 267: empty window, NaN (the sum/nch quirk)
+    fb[7, 4] = 9.0          # clipped outlier
+    fb[:, 6] = 3.0          # constant channel: empty clip, NaN (0/0) as the reference
+    fb[11, :] = 1.5         # constant row: zero-DM count floor
+    a = O.subtract_bp_full(fb)
+    b = _loop_subtract_bp_full(fb)
+    assert np.array_equal(np.isnan(a), np.isnan(b))
+    assert np.isnan(a[:, [3, 6]]).all() and not np.isnan(a[:, [0, 1, 2, 4, 5, 7, 8]]).any()
+    assert np.allclose(a, b, rtol=0, atol=1e-12, equal_nan=True)
+    assert abs(a[:, 2].mean()) < 1e-12  # all rows kept: the plain mean is subtracted
+    z = O.subtract_zero(fb)
+    assert np.allclose(z, _loop_subtract_zero(fb), rtol=0, atol=1e-12)
+    assert np.array_equal(z[11], fb[11])  # sig 0: nothing inside the open interval, mean 0 subtracted

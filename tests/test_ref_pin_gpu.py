@@ -2,7 +2,8 @@
 
 The harness libraries in oracle/_ref (built from the reference sources, see
 oracle/build_ref.py) run the reference's convertarray + cuFFT R2C + sumpower
-+ avepower + per-row copies, subtractbpCAL, dedisperse + calcstats (PIPE),
++ avepower + per-row copies, subtractbpCAL, the dead-code subtractbp and
+subtractZERO, dedisperse + calcstats (PIPE),
 dedisperseSTATS (TS) and the per-channel calcstats (STATS) with the
 reference's launch shapes.  Three-way comparisons: reference vs FP64 oracle
 (pins the oracle), product vs oracle (the parity bar).
@@ -31,6 +32,7 @@ def _lib(tool):
     lib.ref_gpu_channelise.argtypes = [vp, vp, ci, ci, ci, ci, ci, ci, vp, cf]
     lib.ref_gpu_bandpass.argtypes = [vp, ci, ci, cf]
     if tool in ("pipe", "ts"):
+        lib.ref_gpu_subtract_mode.argtypes = [vp, ci, ci, ci, cf]
         lib.ref_gpu_dedisperse.argtypes = [vp, ci, ci, vp, ci, ci, vp, vp, vp, vp, vp, vp, cf]
     if tool == "stats":
         lib.ref_gpu_chanstats.argtypes = [vp, ci, ci, ci, ci, vp, vp, vp, cf]
@@ -91,6 +93,39 @@ def test_bandpass_reference_oracle_product(vf, O, tool):
     assert np.max(np.abs(ref - orc)) <= 2e-5 * scale
     got = vf.bandpass(torch.from_numpy(fb).cuda()).cpu().numpy().T
     assert np.max(np.abs(got - orc)) <= 1e-6 * scale
+
+
+@pytest.mark.parametrize("tool", ["pipe", "ts"])
+@pytest.mark.parametrize("kind", [0, 1])
+def test_subtract_modes_reference_oracle_product(vf, O, tool, kind):
+    """The dead-code modes subtractbp (kind 0) and subtractZERO (kind 1): the
+    reference's kernels, the FP64 oracle and the product."""
+    import torch
+    lib = _lib(tool)
+    rng = np.random.default_rng(30 + kind)
+    maxnt, nch = 1500, 320
+    fb = (rng.standard_normal((maxnt, nch)) * rng.uniform(1, 3, nch)).astype(np.float32)
+    fb[rng.integers(0, maxnt, 50), rng.integers(0, nch, 50)] += 80.0
+    if kind == 0:
+        fb[:, 17] = fb[:, 17] * 30 + 200.0  # wide window about sum/NCHANOUT: every row kept
+        fb[:, 40] = 4.0    # empty clip -> NaN in all three
+    ref = fb.copy()
+    ms = C.c_float(0)
+    assert lib.ref_gpu_subtract_mode(ref.ctypes.data, maxnt, nch, kind, C.byref(ms)) == 0
+    x64 = fb.astype(np.float64)
+    orc = O.subtract_bp_full(x64) if kind == 0 else O.subtract_zero(x64)
+    assert np.array_equal(np.isnan(ref), np.isnan(orc))
+    ok = ~np.isnan(orc)
+    scale = np.abs(fb).max()
+    # the reference sums up to 1500 floats sequentially in FP32
+    e_ref = np.max(np.abs(ref[ok] - orc[ok])) / scale
+    print(f"reference kind {kind} vs FP64: {e_ref:.2e} of max|x| ({ms.value:.2f} ms)")
+    assert e_ref <= 5e-5
+    cm = torch.from_numpy(np.ascontiguousarray(fb.T)).cuda()
+    (vf.subtract_bp_full if kind == 0 else vf.subtract_zero)(cm)
+    got = cm.cpu().numpy().T
+    assert np.array_equal(np.isnan(got), np.isnan(orc))
+    assert np.max(np.abs(got[ok] - orc[ok])) <= 1e-6 * scale
 
 
 def test_dedisperse_calcstats_reference_oracle_product(vf, O):

@@ -74,6 +74,52 @@ def test_pipe_tool_outputs(vf, O, co, tmp_path):
     _close(fil, bp, 5e-5, "nohead.fil (block 4)")
 
 
+def test_pipe_tool_streaming_fil_cands_and_rfi_modes(vf, O, co, tmp_path):
+    """Extensions: -filall streams every block's filterbank into NAME.fil (one
+    continuous series after the header), -cands writes the clustered
+    candidates, -bpfull/-zerodm switch on the reference's dead-code modes."""
+    from vlite_frb_b200 import synth
+    nave, maxtime = 2, 0.2
+    dms = np.arange(0, 5.5, 0.5, dtype=np.float32)
+    with open(tmp_path / "DM101.txt", "w") as f:
+        for d in dms:
+            f.write(f"{d:.1f}\n")
+    spec = synth.StreamSpec(duration=0.9, seed=22, pulses=[synth.Pulse(0.55, 3.0, 2.0, 60.0)])
+    buf = synth.make_vdif(spec).numpy()
+    buf.tofile(tmp_path / "in.vdif")
+    exe = _tool("vdifFILE2dedisp_PIPELINE")
+    base = [exe, "-nchan", "6250", "-nave", str(nave), "-nb", "32", "-i", "in.vdif", "-fullband",
+            "-maxtime", str(maxtime), "-filall"]
+    r = subprocess.run(base + ["-o", "a", "-cands", "8", "-boxcar", "8"], cwd=tmp_path, capture_output=True,
+                       text=True, timeout=600)
+    assert r.returncode == 0, (r.stderr, (tmp_path / "a.log").read_text())
+    r = subprocess.run(base + ["-o", "b", "-bpfull", "-zerodm"], cwd=tmp_path, capture_output=True, text=True,
+                       timeout=600)
+    assert r.returncode == 0, (r.stderr, (tmp_path / "b.log").read_text())
+
+    L = O.Layout(nave=nave, muoslowfreq=384.0, maxtime=maxtime)
+    off, md = O.delay_table(dms, L.fch1, L.chanbw, L.tchan, L.nchanout)
+    h0, bundles, _ = O.read_bundles(buf, L)
+    rows = co.channelise(np.concatenate([b[0] for b in bundles]), np.concatenate([b[1] for b in bundles]), L)
+    blocks = list(O.run_blocks(rows, L, md))
+    assert len(blocks) >= 3
+    hdr = O.sigproc_header(L.fch1, -L.chanbw, L.nchanout, O.vdif_dmjd(h0), nave * 12500 / 128e6)
+    first = (md // L.nbundle) * L.nbundle
+    for name, chain in (("a", co.bandpass), ("b", lambda fb: O.subtract_zero(O.subtract_bp_full(fb)))):
+        raw = (tmp_path / f"{name}.fil").read_bytes()
+        assert raw[:len(hdr)] == hdr
+        got = np.frombuffer(raw[len(hdr):], np.float32).reshape(-1, L.nchanout)
+        want = np.concatenate([chain(fb)[0 if q == 0 else first:] for q, fb in blocks])
+        assert got.shape == want.shape
+        _close(got, want, 5e-5, f"{name}.fil")
+    lines = [ln.split() for ln in (tmp_path / "a.cands").read_text().splitlines() if not ln.startswith("#")]
+    assert lines, "no candidate"
+    best = max(lines, key=lambda v: float(v[3]))
+    t_s, dm = float(best[1]), float(best[2])
+    print("brightest cluster", best)
+    assert abs(t_s - 0.55) < 0.003 and abs(dm - 3.0) <= 1.0
+
+
 def test_pipe_tool_short_input_and_bad_args(vf, tmp_path):
     from vlite_frb_b200 import synth
     exe = _tool("vdifFILE2dedisp_PIPELINE")

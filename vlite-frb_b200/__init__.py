@@ -72,7 +72,7 @@ class BpArgs(C.Structure):
                 ("storage", C.c_int32), ("out", C.c_void_p), ("out_chan_stride", C.c_int64),
                 ("out_row0", C.c_int64), ("out_row_mask", C.c_uint32), ("inv_scale", C.c_void_p),
                 ("q_scale", C.c_float), ("win_mean", C.c_void_p), ("win_var", C.c_void_p), ("tm_out", C.c_void_p),
-                ("tm_row_stride", C.c_int64), ("d_err", C.c_void_p)]
+                ("tm_row_stride", C.c_int64), ("d_err", C.c_void_p), ("subtract_mode", C.c_int32)]
 
 
 class DdArgs(C.Structure):
@@ -111,6 +111,8 @@ _lib.vfrb_dedisperse_workspace_bytes.argtypes = [C.c_void_p, C.c_int64]
 _lib.vfrb_dedisperse.argtypes = [C.c_void_p, C.POINTER(DdArgs), C.c_void_p]
 _lib.vfrb_fb_to_time_major.argtypes = [C.c_void_p, C.c_int64, C.c_int64, C.c_uint32, C.c_int, C.c_int, C.c_void_p,
                                        C.c_int64, C.c_void_p]
+for _n in ("vfrb_subtract_bp_full", "vfrb_subtract_zero"):
+    getattr(_lib, _n).argtypes = [C.c_void_p, C.c_int64, C.c_int64, C.c_uint32, C.c_int, C.c_int64, C.c_void_p]
 
 
 def _check(st: int, what: str):
@@ -187,7 +189,7 @@ def channelise(frames, slots0, slots1, sample0: int, nrows: int, L: Layout, out=
 
 def bandpass(fb_tm, nrows=None, storage=F32, out=None, out_row0=0, out_row_mask=0xFFFFFFFF, inv_scale=None,
              q_scale=16.0, in_row0=0, in_row_mask=0xFFFFFFFF, window=128, win_mean=None, win_var=None,
-             tm_out=None, d_err=None, stream=None):
+             tm_out=None, d_err=None, subtract_mode=0, stream=None):
     torch = _torch()
     nrows = fb_tm.shape[0] if nrows is None else nrows
     nchan = fb_tm.shape[1]
@@ -199,9 +201,27 @@ def bandpass(fb_tm, nrows=None, storage=F32, out=None, out_row0=0, out_row_mask=
                out_chan_stride=out.stride(0), out_row0=out_row0, out_row_mask=out_row_mask,
                inv_scale=_ptr(inv_scale), q_scale=q_scale, win_mean=_ptr(win_mean), win_var=_ptr(win_var),
                tm_out=_ptr(tm_out), tm_row_stride=tm_out.stride(0) if tm_out is not None else 0,
-               d_err=_ptr(d_err))
+               d_err=_ptr(d_err), subtract_mode=subtract_mode)
     _check(_lib.vfrb_bandpass(C.byref(a), _stream(stream)), "vfrb_bandpass")
     return out
+
+
+def _rfi_call(fn, name, fb_cm, nrows, row0, row_mask, stream):
+    if fb_cm.dtype != _torch().float32 or fb_cm.dim() != 2 or fb_cm.stride(1) != 1:
+        raise ValueError(name + ": fb_cm must be a [nchan][rows] float32 tensor with unit row stride")
+    nrows = fb_cm.shape[1] if nrows is None else nrows
+    _check(fn(fb_cm.data_ptr(), fb_cm.stride(0), row0, row_mask, fb_cm.shape[0], nrows, _stream(stream)), name)
+    return fb_cm
+
+
+def subtract_bp_full(fb_cm, nrows=None, row0=0, row_mask=0xFFFFFFFF, stream=None):
+    """In place: subtractbp (whole-block clipped channel mean, PIPE:1372-1424)."""
+    return _rfi_call(_lib.vfrb_subtract_bp_full, "vfrb_subtract_bp_full", fb_cm, nrows, row0, row_mask, stream)
+
+
+def subtract_zero(fb_cm, nrows=None, row0=0, row_mask=0xFFFFFFFF, stream=None):
+    """In place: subtractZERO (per-row clipped mean across channels, PIPE:1478-1515)."""
+    return _rfi_call(_lib.vfrb_subtract_zero, "vfrb_subtract_zero", fb_cm, nrows, row0, row_mask, stream)
 
 
 class DedispPlan:
@@ -312,6 +332,7 @@ def fb_to_time_major(fb_cm, nrows=None, row0=0, row_mask=0xFFFFFFFF, out=None, s
 MODE_BLOCK, MODE_STREAM = 0, 1
 READER_PIPE, READER_TS = 0, 1
 OUT_DEDISP, OUT_DMSTATS, OUT_SIGMA, OUT_CHANSTATS, OUT_FB, OUT_CANDS = 1, 2, 4, 8, 16, 32
+BP_CAL, BP_FULL = 0, 1
 VFRB_PENDING = 9
 
 
@@ -322,7 +343,8 @@ class Params(C.Structure):
                 ("dada_skip", C.c_int32), ("storage", C.c_int32), ("q_scale", C.c_float), ("outputs", C.c_int32),
                 ("fb_block", C.c_int32), ("nstreams", C.c_int32), ("chunk_seconds", C.c_float),
                 ("ring_seconds", C.c_float), ("cand_snr", C.c_float), ("device", C.c_int32),
-                ("device_bytes", C.c_int64), ("boxcar_max", C.c_int32)]
+                ("device_bytes", C.c_int64), ("boxcar_max", C.c_int32), ("bp_mode", C.c_int32),
+                ("zero_dm", C.c_int32)]
 
 
 class Cand(C.Structure):
@@ -339,6 +361,27 @@ class Result(C.Structure):
                 ("chan_outlier", C.c_void_p), ("ncand", C.c_int32), ("cands", C.c_void_p),
                 ("latency_ms", C.c_double), ("device_errors", C.c_int32), ("box_snr", C.c_void_p),
                 ("box_start", C.c_void_p), ("box_width", C.c_void_p)]
+
+
+_lib.vfrb_cluster_cands.argtypes = [C.POINTER(Cand), C.c_int32, C.c_int32, C.c_int64, C.POINTER(Cand),
+                                    C.POINTER(C.c_int32), C.c_void_p]
+
+
+def cluster_cands(cands, dm_tol=2, t_tol=0):
+    """Friends-of-friends clustering of candidate dicts (dm_index, t, width,
+    snr, dm) across trials and time (vfrb_cluster_cands).  Returns
+    (clusters, labels): one dict per cluster -- its brightest member -- and
+    the cluster index of each input."""
+    n = len(cands)
+    arr = (Cand * max(n, 1))()
+    for i, c in enumerate(cands):
+        arr[i] = Cand(dm_index=c["dm_index"], width=c["width"], t=c["t"], snr=c["snr"], dm=c.get("dm", 0.0))
+    out = (Cand * max(n, 1))()
+    nout = C.c_int32(0)
+    lab = np.zeros(max(n, 1), np.int32)
+    _check(_lib.vfrb_cluster_cands(arr, n, dm_tol, t_tol, out, C.byref(nout), lab.ctypes.data), "vfrb_cluster_cands")
+    cl = [dict(dm_index=o.dm_index, width=o.width, t=o.t, snr=o.snr, dm=o.dm) for o in out[:nout.value]]
+    return cl, lab[:n]
 
 
 _lib.vfrb_params_default.argtypes = [C.POINTER(Params)]

@@ -27,8 +27,8 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC,-Wall,-Wno-unused-function",
           "--expt-relaxed-constexpr", "-I" + os.path.join(REPO, "include"), "-I" + CSRC]
 
-LIB_SOURCES = ["channelise.cu", "bandpass.cu", "dedisperse.cu", "vfrb_api.cpp"]
-LIB_SOURCES_OPTIONAL = ["engine.cu", "vdif_reader.cpp", "writers.cpp", "dada.cpp", "noalloc.cu", "candidates.cu"]
+LIB_SOURCES = ["channelise.cu", "bandpass.cu", "rfi.cu", "dedisperse.cu", "vfrb_api.cpp"]
+LIB_SOURCES_OPTIONAL = ["engine.cu", "vdif_reader.cpp", "writers.cpp", "dada.cpp", "noalloc.cu", "candidates.cu", "cluster.cpp"]
 TOOL_MAINS = ["vdifFILE2dedisp_PIPELINE.cpp", "vdifDADA2stats.cpp", "vdifDADA2timeseries.cpp", "vfrb_dada_write.cpp"]
 
 

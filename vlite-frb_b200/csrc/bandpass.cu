@@ -8,7 +8,9 @@
 // reference calls "sig", the open-interval clip ave +- 3 sig and the clipped
 // mean (count floored at 1).  The subtracted rows are written channel-major
 // (512-byte runs per channel), the layout the dedisperser streams, in FP32,
-// FP16 (z = x/s_c) or int8 (round(z*q)) form.
+// FP16 (z = x/s_c) or int8 (round(z*q)) form.  subtract_mode 1 skips the
+// statistics and writes the rows unchanged (the input of the whole-block
+// subtractbp in rfi.cu).
 #include "vfrb_common.cuh"
 
 namespace vfrb {
@@ -57,37 +59,40 @@ __global__ void __launch_bounds__(kBpThreads) k_bandpass(const vfrb_bp_args a) {
       x[k] = (r < npts) ? tile[cl][r] : 0.f;
       s += (r < npts) ? (double)x[k] : 0.0;
     }
-    const double n = (double)npts;
-    const double ave = warp_sum(s) / n;
-    double sd = 0.0, sd2 = 0.0;
+    double cave = 0.0, sig = 0.0;  // subtract_mode 1: copy only (cave = 0)
+    if (a.subtract_mode == 0) {
+      const double n = (double)npts;
+      const double ave = warp_sum(s) / n;
+      double sd = 0.0, sd2 = 0.0;
 #pragma unroll
-    for (int k = 0; k < kBpMaxWin / 32; ++k) {
-      const int r = lane + 32 * k;
-      if (r < npts) {
-        const double d = (double)x[k] - ave;
-        sd += d;
-        sd2 += d * d;
+      for (int k = 0; k < kBpMaxWin / 32; ++k) {
+        const int r = lane + 32 * k;
+        if (r < npts) {
+          const double d = (double)x[k] - ave;
+          sd += d;
+          sd2 += d * d;
+        }
       }
-    }
-    sd = warp_sum(sd);
-    sd2 = warp_sum(sd2);
-    const double sig = (sd2 - (sd * sd) / n) / (n - 1.0);  // variance, NaN when npts == 1
-    const double hi = ave + 3.0 * sig, lo = ave - 3.0 * sig;
-    double cs = 0.0;
-    int cnt = 0;
+      sd = warp_sum(sd);
+      sd2 = warp_sum(sd2);
+      sig = (sd2 - (sd * sd) / n) / (n - 1.0);  // variance, NaN when npts == 1
+      const double hi = ave + 3.0 * sig, lo = ave - 3.0 * sig;
+      double cs = 0.0;
+      int cnt = 0;
 #pragma unroll
-    for (int k = 0; k < kBpMaxWin / 32; ++k) {
-      const int r = lane + 32 * k;
-      const double xv = (double)x[k];
-      if (r < npts && xv < hi && xv > lo) {
-        cs += xv;
-        ++cnt;
+      for (int k = 0; k < kBpMaxWin / 32; ++k) {
+        const int r = lane + 32 * k;
+        const double xv = (double)x[k];
+        if (r < npts && xv < hi && xv > lo) {
+          cs += xv;
+          ++cnt;
+        }
       }
+      cs = warp_sum(cs);
+      cnt = warp_sum_i(cnt);
+      if (cnt == 0) cnt = 1;
+      cave = cs / (double)cnt;
     }
-    cs = warp_sum(cs);
-    cnt = warp_sum_i(cnt);
-    if (cnt == 0) cnt = 1;
-    const double cave = cs / (double)cnt;
     if (lane == 0) {
       if (a.win_mean) a.win_mean[(long long)win * a.nchan + c] = (float)cave;
       if (a.win_var) a.win_var[(long long)win * a.nchan + c] = (float)sig;
@@ -128,6 +133,7 @@ int launch_bandpass(const vfrb_bp_args& a, cudaStream_t s) {
   if (a.nrows <= 0) return a.nrows == 0 ? VFRB_OK : VFRB_ERR_ARG;
   if (!a.in || !a.out || a.nchan <= 0 || a.window <= 0 || a.window > kBpMaxWin) return VFRB_ERR_ARG;
   if (a.storage != VFRB_F32 && !a.inv_scale) return VFRB_ERR_ARG;
+  if (a.subtract_mode != 0 && a.subtract_mode != 1) return VFRB_ERR_ARG;
   const int nwin = (a.nrows + a.window - 1) / a.window;
   dim3 grid((a.nchan + kBpChan - 1) / kBpChan, nwin);
   switch (a.storage) {

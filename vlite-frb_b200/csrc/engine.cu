@@ -446,7 +446,7 @@ int init_scale(vfrb_plan* pl, StreamSt* s, const float* raw, int64_t row0, unsig
 }
 
 int run_bandpass(vfrb_plan* pl, StreamSt* s, const float* raw, int64_t in_row0, unsigned in_mask, int64_t nrows,
-                 int64_t out_row0, float* tm_out) {
+                 int64_t out_row0, float* tm_out, int subtract_mode = 0) {
   ST(init_scale(pl, s, raw, in_row0, in_mask));
   vfrb_bp_args a{};
   a.in = raw;
@@ -466,6 +466,7 @@ int run_bandpass(vfrb_plan* pl, StreamSt* s, const float* raw, int64_t in_row0, 
   a.tm_out = tm_out;
   a.tm_row_stride = pl->L.nchanout;
   a.d_err = s->d_err;
+  a.subtract_mode = subtract_mode;
   return launch_bandpass(a, s->cs);
 }
 
@@ -579,7 +580,18 @@ int block_complete(vfrb_plan* pl, StreamSt* s) {
     CK(cudaMemcpyAsync(s->d_left, s->d_fb_tm + (int64_t)(L.maxnt - pl->max_delay) * nch,
                        (size_t)pl->max_delay * nch * 4, cudaMemcpyDeviceToDevice, s->cs));
   const bool with_fb = want(pl, VFRB_OUT_FB) && (pl->P.fb_block < 0 || pl->P.fb_block == s->blocks);
-  ST(run_bandpass(pl, s, s->d_fb_tm, 0, 0xffffffffu, L.maxnt, 0, with_fb ? s->d_fbt : nullptr));
+  const bool full_bp = pl->P.bp_mode == VFRB_BP_FULL;
+  if (!full_bp && !pl->P.zero_dm) {
+    ST(run_bandpass(pl, s, s->d_fb_tm, 0, 0xffffffffu, L.maxnt, 0, with_fb ? s->d_fbt : nullptr));
+  } else {
+    // subtractbp (whole block, PIPE:1372) in place of subtractbpCAL, and/or
+    // subtractZERO after it (PIPE:661): in place on the FP32 block
+    ST(run_bandpass(pl, s, s->d_fb_tm, 0, 0xffffffffu, L.maxnt, 0, nullptr, full_bp ? 1 : 0));
+    float* cm = (float*)s->d_cm;
+    if (full_bp) ST(launch_subtract_bp_full(cm, s->cm_stride, 0, 0xffffffffu, (int)nch, L.maxnt, s->cs));
+    if (pl->P.zero_dm) ST(launch_subtract_zero(cm, s->cm_stride, 0, 0xffffffffu, (int)nch, L.maxnt, s->cs));
+    if (with_fb) ST(launch_fb_transpose(cm, s->cm_stride, 0xffffffffu, 0, (int)nch, L.maxnt, s->d_fbt, nch, s->cs));
+  }
   if (want(pl, VFRB_OUT_CHANSTATS)) {
     vfrb_cs_args c{};
     c.fb = (const float*)s->d_cm;
@@ -595,7 +607,13 @@ int block_complete(vfrb_plan* pl, StreamSt* s) {
     ST(launch_chan_stats(c, s->cs));
   }
   if (pl->want_dd) ST(run_dedisp(pl, s, 0, L.maxnt, pl->nt_block, true));
-  ST(emit(pl, s, s->blocks, s->blocks, pl->want_dd ? pl->nt_block : 0, with_fb));
+  // absolute FB row of block row 0: block 0 starts at row 0; each later block
+  // begins with the previous block's last max_delay rows, and its new rows
+  // (from row `first` on) follow the previous block's last row
+  const int64_t first = (int64_t)(pl->max_delay / L.nbundle) * L.nbundle;
+  const int64_t row0 =
+      s->blocks == 0 ? 0 : (int64_t)L.maxnt - pl->max_delay + (s->blocks - 1) * ((int64_t)L.maxnt - first);
+  ST(emit(pl, s, s->blocks, row0, pl->want_dd ? pl->nt_block : 0, with_fb));
   if (pl->want_dd && pl->max_delay > 0) {
     CK(cudaMemcpyAsync(s->d_fb_tm, s->d_left, (size_t)pl->max_delay * nch * 4, cudaMemcpyDeviceToDevice, s->cs));
     s->loopcnt = pl->max_delay / L.nbundle;
@@ -936,8 +954,13 @@ int vfrb_plan_create(vfrb_plan** out, const vfrb_params* prm) {
   };
   if (P.nstreams < 1 || P.nstreams > 4096 || (P.mode != VFRB_MODE_BLOCK && P.mode != VFRB_MODE_STREAM) ||
       P.storage < VFRB_F32 || P.storage > VFRB_I8 || P.ring_seconds <= 0.f || P.q_scale <= 0.f ||
-      P.boxcar_max < 0 || P.boxcar_max > 65536)
+      P.boxcar_max < 0 || P.boxcar_max > 65536 || (P.bp_mode != VFRB_BP_CAL && P.bp_mode != VFRB_BP_FULL) ||
+      (P.zero_dm != 0 && P.zero_dm != 1))
     return fail(VFRB_ERR_ARG);
+  // the whole-block bandpass and zero-DM modes work in place on the FP32
+  // channel-major block
+  if ((P.bp_mode == VFRB_BP_FULL || P.zero_dm) && (P.mode != VFRB_MODE_BLOCK || P.storage != VFRB_F32))
+    return fail(VFRB_ERR_UNSUPPORTED);
   if (cudaSetDevice(P.device) != cudaSuccess) return fail(VFRB_ERR_CUDA);
   int st = vfrb_layout_init(&pl->L, P.twonchan, P.nave, P.nbundle, P.muoslowfreq, P.nchanout_fixed, P.maxtime);
   if (st) return fail(st);
@@ -1095,6 +1118,14 @@ int vfrb_poll(vfrb_plan* pl, vfrb_result* out, int wait) {
     // kept where it is a local maximum over neighbouring trials
     const bool box = o.box_snr && o.box_start && o.box_width;
     const float* best = box ? o.box_snr : o.peak;
+    // block mode: rows from `first` on were read after the carried rows
+    // [first, max_delay) that they overwrote, so they sit max_delay - first
+    // rows later in the stream than their block index says
+    const bool blk = pl->P.mode == VFRB_MODE_BLOCK;
+    const int64_t first = (int64_t)(pl->max_delay / pl->L.nbundle) * pl->L.nbundle;
+    auto abs_row = [&](int64_t i) {
+      return o.row0 + i + ((blk && o.seq > 0 && i >= first) ? (int64_t)pl->max_delay - first : 0);
+    };
     for (int d = 0; d < o.ndm; ++d) {
       const float p = best[d];
       if (!(p >= pl->P.cand_snr)) continue;
@@ -1103,7 +1134,7 @@ int vfrb_poll(vfrb_plan* pl, vfrb_result* out, int wait) {
       vfrb_cand c;
       c.dm_index = d;
       c.width = box ? o.box_width[d] : 1;
-      c.t = o.row0 + (box ? o.box_start[d] : o.argmax[d]);
+      c.t = abs_row(box ? o.box_start[d] : o.argmax[d]);
       c.snr = p;
       c.dm = pl->dms[d];
       r->cands.push_back(c);

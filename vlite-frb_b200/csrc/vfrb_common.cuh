@@ -30,5 +30,9 @@ int launch_bandpass(const vfrb_bp_args& a, cudaStream_t s);
 int launch_chan_stats(const vfrb_cs_args& a, cudaStream_t s);
 int launch_fb_transpose(const float* src_cm, long long chan_stride, unsigned row_mask, long long row0,
                         int nchan, int nrows, float* dst_tm, long long dst_row_stride, cudaStream_t s);
+int launch_subtract_bp_full(float* fb, long long chan_stride, long long row0, unsigned row_mask, int nchan,
+                            long long nrows, cudaStream_t s);
+int launch_subtract_zero(float* fb, long long chan_stride, long long row0, unsigned row_mask, int nchan,
+                         long long nrows, cudaStream_t s);
 
 }  // namespace vfrb

@@ -17,7 +17,15 @@
 // Extensions (not in the reference; the reference fixes these at compile
 // time): -fullband (MUOSLOWFREQ 384 MHz: all 6250 channels), -maxtime S
 // (block length, default 70 s), -dmfile PATH (default DM101.txt),
-// -fp16 (FP16 storage form of the filterbank for dedispersion).
+// -fp16 (FP16 storage form of the filterbank for dedispersion),
+// -filall (NAME.fil: SIGPROC header + the bandpassed filterbank of every
+// block, appended as each block completes; block 0 whole, later blocks from
+// row (max_delay/NBUNDLE)*NBUNDLE, the first row the reader refilled, so the
+// file is one continuous time series), -bpfull / -zerodm (the reference's
+// commented-out subtractbp, PIPE:1372, and subtractZERO, PIPE:1478),
+// -cands SNR [-boxcar W] (NAME.cands: per block the trials whose best
+// boxcar SNR reaches SNR and is a local maximum over trials, clustered
+// across trials and blocks; one text line per cluster).
 #include "tool_common.h"
 
 namespace {
@@ -29,6 +37,9 @@ struct Opts {
   float maxtime = 70.f;
   std::string dmfile = "DM101.txt";
   bool fp16 = false;
+  bool filall = false, bpfull = false, zerodm = false;
+  float cand_snr = 0.f;  // 0: no candidate file
+  int boxcar = 1;
 };
 
 void usage() {
@@ -47,7 +58,12 @@ void usage() {
                "\t             -fullband      write the full 320-384 MHz band (MUOSLOWFREQ 384)\n"
                "\t             -maxtime (s)   block length (default 70)\n"
                "\t             -dmfile (path) DM trial list (default DM101.txt)\n"
-               "\t             -fp16          FP16 storage form for dedispersion\n\n"
+               "\t             -fp16          FP16 storage form for dedispersion\n"
+               "\t             -filall        write every block's filterbank to NAME.fil (with header)\n"
+               "\t             -bpfull        whole-block bandpass (subtractbp) instead of cal windows\n"
+               "\t             -zerodm        subtract the zero-DM signal (subtractZERO)\n"
+               "\t             -cands (float) write clustered candidates above this SNR to NAME.cands\n"
+               "\t             -boxcar (int)  widest boxcar of the candidate search (default 1)\n\n"
                "  DEFAULTS:\n"
                "\t             -o     testDEDISP\n"
                "\t             -nave  4\n"
@@ -85,6 +101,16 @@ int parse(int argc, char** argv, Opts& o) {
       o.dmfile = argv[++i];
     } else if (tool::eq(argv[i], "-fp16")) {
       o.fp16 = true;
+    } else if (tool::eq(argv[i], "-filall")) {
+      o.filall = true;
+    } else if (tool::eq(argv[i], "-bpfull")) {
+      o.bpfull = true;
+    } else if (tool::eq(argv[i], "-zerodm")) {
+      o.zerodm = true;
+    } else if (tool::eq(argv[i], "-cands") && more) {
+      o.cand_snr = (float)std::atof(argv[++i]);
+    } else if (tool::eq(argv[i], "-boxcar") && more) {
+      o.boxcar = std::atoi(argv[++i]);
     } else {
       std::fprintf(stderr, "Error! Unknown argument: %s\n\n", argv[i]);
       usage();
@@ -140,8 +166,25 @@ int main(int argc, char** argv) {
   p.mode = VFRB_MODE_BLOCK;
   p.reader = VFRB_READER_PIPE;
   p.outputs = VFRB_OUT_DEDISP | VFRB_OUT_DMSTATS | VFRB_OUT_FB;
-  p.fb_block = 4;  // the block the reference copies out (q == 4)
+  p.fb_block = o.filall ? -1 : 4;  // the block the reference copies out (q == 4), or all
   p.storage = o.fp16 ? VFRB_F16 : VFRB_F32;
+  p.bp_mode = o.bpfull ? VFRB_BP_FULL : VFRB_BP_CAL;
+  p.zero_dm = o.zerodm ? 1 : 0;
+  if (o.cand_snr > 0.f) {
+    p.outputs |= VFRB_OUT_CANDS;
+    p.cand_snr = o.cand_snr;
+    p.boxcar_max = o.boxcar;
+  }
+  FILE* filall = nullptr;
+  if (o.filall) {
+    const std::string n = o.out + ".fil";
+    if (tool::file_exists(n.c_str())) std::remove(n.c_str());
+    filall = std::fopen(n.c_str(), "wb");
+    if (!filall) {
+      std::fprintf(stderr, "Unable to open output SIGPROC filterbank file: %s\n", n.c_str());
+      return 2;
+    }
+  }
 
   tool::Source src;
   if (o.in.empty() || !src.open(o.in.c_str())) {
@@ -178,6 +221,8 @@ int main(int argc, char** argv) {
   std::vector<float> keep_dd((size_t)dms.size() * (size_t)std::max<int64_t>(ntime_outdd, 0), 0.f);
   std::vector<float> keep_fb((size_t)L.maxnt * L.nchanout, 0.f);
   int64_t nblocks = 0;
+  bool files_ok = true;
+  std::vector<vfrb_cand> cands;
   const double tsamp = (double)L.nave * L.twonchan / 128e6;
   st = tool::run_stream(
       plan, src, log,
@@ -185,6 +230,7 @@ int main(int argc, char** argv) {
         std::vector<uint8_t> h(vfrb_sigproc_header(nullptr, 0, L.fch1, L.foff, L.nchanout, 32, mjd, tsamp, 1));
         vfrb_sigproc_header(h.data(), h.size(), L.fch1, L.foff, L.nchanout, 32, mjd, tsamp, 1);
         tool::write_all(head, h.data(), h.size());
+        if (filall) files_ok = tool::write_all(filall, h.data(), h.size()) && files_ok;
       },
       [&](const vfrb_result& r) {
         std::fprintf(log, "block %lld: %lld samples x %d DM trials, device errors %d\n", (long long)r.seq,
@@ -193,8 +239,33 @@ int main(int argc, char** argv) {
           if (r.dd && r.nt == ntime_outdd) std::memcpy(keep_dd.data(), r.dd, keep_dd.size() * 4);
           if (r.fb && r.fb_rows == L.maxnt) std::memcpy(keep_fb.data(), r.fb, keep_fb.size() * 4);
         }
+        if (filall && r.fb && r.fb_rows == L.maxnt) {
+          const int64_t first = r.seq == 0 ? 0 : (int64_t)(max_delay / L.nbundle) * L.nbundle;
+          files_ok = tool::write_all(filall, r.fb + (size_t)first * L.nchanout,
+                                     (size_t)(L.maxnt - first) * L.nchanout * 4) && files_ok;
+        }
+        for (int32_t k = 0; k < r.ncand; ++k) cands.push_back(r.cands[k]);
         ++nblocks;
       });
+  if (filall) std::fclose(filall);
+  if (o.cand_snr > 0.f) {
+    // one pulse: within 8 trials and 50 samples
+    std::vector<vfrb_cand> cl(cands.size());
+    int32_t ncl = 0;
+    vfrb_cluster_cands(cands.data(), (int32_t)cands.size(), 8, 50, cl.data(), &ncl, nullptr);
+    FILE* cf = std::fopen((o.out + ".cands").c_str(), "w");
+    if (cf) {
+      std::fprintf(cf, "# sample  time_s  dm  snr  width  dm_index\n");
+      for (int32_t k = 0; k < ncl; ++k)
+        std::fprintf(cf, "%lld %.6f %.3f %.3f %d %d\n", (long long)cl[(size_t)k].t, cl[(size_t)k].t * tsamp,
+                     (double)cl[(size_t)k].dm, (double)cl[(size_t)k].snr, cl[(size_t)k].width,
+                     cl[(size_t)k].dm_index);
+      std::fclose(cf);
+    } else {
+      files_ok = false;
+    }
+    std::fprintf(log, "%d candidates in %d clusters\n", (int)cands.size(), (int)ncl);
+  }
   // OUTDD.bin (PIPE:734-739) and the headerless filterbank (PIPE:777)
   for (size_t i = 0; i < dms.size(); ++i) {
     tool::write_all(outdd, &dms[i], 4);
@@ -207,6 +278,10 @@ int main(int argc, char** argv) {
   std::fclose(outdd);
   vfrb_plan_destroy(plan);
   std::fprintf(log, "Processed %lld blocks (q= %lld)\n", (long long)nblocks, (long long)nblocks);
+  if (!files_ok) {
+    std::fprintf(log, "Error writing the output files\n");
+    if (st == 0) st = 2;
+  }
   const double t = tool::now_s() - t_begin;
   std::fprintf(log, "Total run time = %f [sec]\n", t);
   std::fprintf(log, "\nfinished!\n");
