@@ -228,37 +228,42 @@ __global__ void __launch_bounds__(kPatWarps * 32, 2) k_dedisp_pat(const DdPatPar
   const unsigned long long rmask = (unsigned long long)p.row_mask;
   int err = 0;
   if (tid == 0) {
-    mbar_init(&s_full[0], 1);
-    mbar_init(&s_full[1], 1);
+    mbar_init(&s_full[0], kPatWarps);
+    mbar_init(&s_full[1], kPatWarps);
     mbar_fence_init();
   }
   __syncthreads();
 
-  // Producer (warp 0): chunk k's rows into tile buffer b.  A channel's rows
-  // [a, a + LM) go in one bulk asynchronous copy when they are all valid (two
-  // when they wrap the ring: the split is at the ring end, a multiple of 16
-  // bytes); otherwise the warp copies them itself, with zeros outside
-  // [0, row0 + nrows_valid), before announcing the bulk bytes.
+  // Staging, shared by the eight warps: warp w copies its ceil(CH/8)
+  // channels of chunk k into tile buffer b.  A channel's rows [a, a + LM) go
+  // in one bulk asynchronous copy when they are all valid (two when they
+  // wrap the ring: the split is at the ring end, a multiple of 16 bytes);
+  // otherwise the warp copies them itself, with zeros outside
+  // [0, row0 + nrows_valid), before announcing its bulk bytes.  Each warp
+  // arrives once per buffer phase, so the barrier counts eight arrivals.
+  const int per = (CH + kPatWarps - 1) / kPatWarps;
   auto stage = [&](int k, int b) {
     const int c0 = k * CH;
     const int nc = min(CH, p.nchan - c0);
+    const int cb = warp * per;                 // this warp's first channel of the chunk
+    const int cn = max(0, min(per, nc - cb));  // and how many
     long long a = 0;
     unsigned long long ra = 0;
     int n1 = LM;  // rows before the ring end
     bool bulk = false;
-    if (lane < nc) {
-      a = (p.row0 + t0 + __ldg(p.bmin + (long long)blk * p.nchan + c0 + lane)) & ~(long long)(VEC - 1);
+    if (lane < cn) {
+      a = (p.row0 + t0 + __ldg(p.bmin + (long long)blk * p.nchan + c0 + cb + lane)) & ~(long long)(VEC - 1);
       ra = (unsigned long long)a & rmask;
       bulk = a >= 0 && a + LM <= vend;
       if (ra + (unsigned long long)LM > rmask + 1ULL) n1 = (int)(rmask + 1ULL - ra);
     }
-    unsigned slow = __ballot_sync(0xffffffffu, lane < nc && !bulk);
+    unsigned slow = __ballot_sync(0xffffffffu, lane < cn && !bulk);
     while (slow) {
       const int cl = __ffs(slow) - 1;
       slow &= slow - 1;
       const long long ac = __shfl_sync(0xffffffffu, a, cl);
-      const T* src = fb + (long long)(c0 + cl) * p.chan_stride;
-      int4* dst = tiles + ((long long)b * CH + cl) * LMQ;
+      const T* src = fb + (long long)(c0 + cb + cl) * p.chan_stride;
+      int4* dst = tiles + ((long long)b * CH + cb + cl) * LMQ;
       for (int v = lane; v < LMQ; v += 32) {
         const long long r = ac + (long long)v * VEC;
         int4 val = make_int4(0, 0, 0, 0);
@@ -286,8 +291,8 @@ __global__ void __launch_bounds__(kPatWarps * 32, 2) k_dedisp_pat(const DdPatPar
     if (lane == 0) mbar_arrive_expect_tx(&s_full[b], nbulk * (unsigned)(LM * (int)sizeof(T)));
     __syncwarp();
     if (bulk) {
-      int4* dst = tiles + ((long long)b * CH + lane) * LMQ;
-      const T* src = fb + (long long)(c0 + lane) * p.chan_stride;
+      int4* dst = tiles + ((long long)b * CH + cb + lane) * LMQ;
+      const T* src = fb + (long long)(c0 + cb + lane) * p.chan_stride;
       bulk_g2s(dst, src + ra, (unsigned)(n1 * (int)sizeof(T)), &s_full[b]);
       if (n1 < LM) bulk_g2s(dst + n1 / VEC, src, (unsigned)((LM - n1) * (int)sizeof(T)), &s_full[b]);
     }
@@ -343,10 +348,10 @@ __global__ void __launch_bounds__(kPatWarps * 32, 2) k_dedisp_pat(const DdPatPar
 #pragma unroll
     for (int i = 0; i < TT; ++i) acc[j][i] = 0.f;
 
-  if (warp == 0) stage(0, 0);
+  stage(0, 0);
   for (int k = 0; k < nchunks; ++k) {
     __syncthreads();  // every warp is done with chunk k-1: its buffer can be refilled
-    if (warp == 0 && k + 1 < nchunks) stage(k + 1, (k + 1) & 1);
+    if (k + 1 < nchunks) stage(k + 1, (k + 1) & 1);
     meta(k);
     if (!mbar_wait(&s_full[k & 1], (unsigned)(k >> 1) & 1u)) err |= kErrTimeout;
     const int b = k & 1;
