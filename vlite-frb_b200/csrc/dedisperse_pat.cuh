@@ -89,9 +89,13 @@ template <typename T, int D, int TT, int... S>
 __device__ __forceinline__ void pat_run(float (&acc)[D][TT], const T* tile, const int* slot, int n, int lane_off) {
   constexpr int NW = TT + PatMax<S...>::v;
   using R = typename PatElem<T>::R;
+  // slot[n] (read ahead on the last channel) is the next entry of the same
+  // shared table, in bounds and unused
+  int sl = slot[0];
 #pragma unroll 1
   for (int i = 0; i < n; ++i) {
-    const T* src = tile + slot[i] + lane_off;
+    const T* src = tile + sl + lane_off;
+    sl = slot[i + 1];
     R w[NW];
 #pragma unroll
     for (int k = 0; k < NW; ++k) w[k] = PatElem<T>::load(src + k);
@@ -242,7 +246,15 @@ __global__ void __launch_bounds__(kPatWarps * 32, 2) k_dedisp_pat(const DdPatPar
   // [0, row0 + nrows_valid), before announcing its bulk bytes.  Each warp
   // arrives once per buffer phase, so the barrier counts eight arrivals.
   const int per = (CH + kPatWarps - 1) / kPatWarps;
-  auto stage = [&](int k, int b) {
+  // bmin of this lane's staging channel of chunk k (loaded ahead of use)
+  auto stage_bmin = [&](int k) -> int {
+    if (k >= nchunks) return 0;
+    const int c0 = k * CH;
+    const int cb = warp * per;
+    const int cn = max(0, min(per, min(CH, p.nchan - c0) - cb));
+    return lane < cn ? __ldg(p.bmin + (long long)blk * p.nchan + c0 + cb + lane) : 0;
+  };
+  auto stage = [&](int k, int b, int sbmin) {
     const int c0 = k * CH;
     const int nc = min(CH, p.nchan - c0);
     const int cb = warp * per;                 // this warp's first channel of the chunk
@@ -252,7 +264,7 @@ __global__ void __launch_bounds__(kPatWarps * 32, 2) k_dedisp_pat(const DdPatPar
     int n1 = LM;  // rows before the ring end
     bool bulk = false;
     if (lane < cn) {
-      a = (p.row0 + t0 + __ldg(p.bmin + (long long)blk * p.nchan + c0 + cb + lane)) & ~(long long)(VEC - 1);
+      a = (p.row0 + t0 + sbmin) & ~(long long)(VEC - 1);
       ra = (unsigned long long)a & rmask;
       bulk = a >= 0 && a + LM <= vend;
       if (ra + (unsigned long long)LM > rmask + 1ULL) n1 = (int)(rmask + 1ULL - ra);
@@ -299,23 +311,40 @@ __global__ void __launch_bounds__(kPatWarps * 32, 2) k_dedisp_pat(const DdPatPar
   };
 
   // This warp's channels of chunk k, sorted into runs of one pattern.
-  auto meta = [&](int k) {
+  // The per-(group, channel) tables of chunk k for this lane's channel,
+  // loaded one chunk ahead so that their global-load latency hides under the
+  // previous chunk's sums.
+  struct MetaIn {
+    int bmin, gbase, pat;
+    unsigned pk;
+  };
+  auto meta_in = [&](int k) -> MetaIn {
+    MetaIn m{0, 0, 0, 0u};
+    if (k < nchunks && lane < min(CH, p.nchan - k * CH)) {
+      const int c = k * CH + lane;
+      m.bmin = __ldg(p.bmin + (long long)blk * p.nchan + c);
+      m.gbase = __ldg(p.gbase + (long long)g * p.nchan + c);
+      m.pk = __ldg(p.gpack + (long long)g * p.nchan + c);
+      m.pat = __ldg(p.gpat + (long long)g * p.nchan + c);
+    }
+    return m;
+  };
+  auto meta = [&](int k, const MetaIn& m) {
     const int c0 = k * CH;
     const int nc = min(CH, p.nchan - c0);
     int pat = 0x10000 + lane;  // inactive lanes: a pattern of their own
     int slot = 0;
     unsigned pk = 0;
     if (lane < nc) {
-      const int c = c0 + lane;
-      const long long a0 = (p.row0 + t0 + __ldg(p.bmin + (long long)blk * p.nchan + c)) & ~(long long)(VEC - 1);
-      int rel = (int)(p.row0 + t0 + __ldg(p.gbase + (long long)g * p.nchan + c) - a0);
+      const long long a0 = (p.row0 + t0 + m.bmin) & ~(long long)(VEC - 1);
+      int rel = (int)(p.row0 + t0 + m.gbase - a0);
       if (rel < 0 || rel + NT + SMAX > LM) {  // cannot happen with a consistent plan
         err |= kErrOffsetRange;
         rel = 0;
       }
       slot = lane * LM + rel;
-      pk = __ldg(p.gpack + (long long)g * p.nchan + c);
-      pat = __ldg(p.gpat + (long long)g * p.nchan + c);
+      pk = m.pk;
+      pat = m.pat;
     }
     const unsigned same = __match_any_sync(0xffffffffu, pat);
     const int leader = __ffs(same) - 1;
@@ -348,11 +377,15 @@ __global__ void __launch_bounds__(kPatWarps * 32, 2) k_dedisp_pat(const DdPatPar
 #pragma unroll
     for (int i = 0; i < TT; ++i) acc[j][i] = 0.f;
 
-  stage(0, 0);
+  stage(0, 0, stage_bmin(0));
+  int sb_next = stage_bmin(1);
+  MetaIn m_cur = meta_in(0);
   for (int k = 0; k < nchunks; ++k) {
     __syncthreads();  // every warp is done with chunk k-1: its buffer can be refilled
-    if (k + 1 < nchunks) stage(k + 1, (k + 1) & 1);
-    meta(k);
+    if (k + 1 < nchunks) stage(k + 1, (k + 1) & 1, sb_next);
+    sb_next = stage_bmin(k + 2);
+    meta(k, m_cur);
+    m_cur = meta_in(k + 1);
     if (!mbar_wait(&s_full[k & 1], (unsigned)(k >> 1) & 1u)) err |= kErrTimeout;
     const int b = k & 1;
     const T* tile = reinterpret_cast<const T*>(tiles + (long long)b * CH * LMQ);
