@@ -262,6 +262,17 @@ typedef struct vfrb_cs_args {
 } vfrb_cs_args;
 int vfrb_chan_stats(const vfrb_cs_args* a, void* stream);
 
+/* Spectral kurtosis per (channel, block of ncolstatblk rows) of the RAW
+ * time-major FB (before bandpass subtraction; no reference counterpart --
+ * the reference's stats tool has none): the generalised estimator
+ *   SK = (M*nsum + 1)/(M - 1) * (M*S2/S1^2 - 1),
+ * M = rows in the block, S1 = sum x, S2 = sum x^2 (FP64), nsum = raw power
+ * values summed per FB sample (2 pols x NAVE).  E[SK] = 1 for Gaussian
+ * noise.  sk is [nstatblks][nchan]; every block needs a row (one row:
+ * inf/NaN). */
+int vfrb_chan_sk(const float* fb_tm, int64_t row_stride, int nchan, int nrows, int ncolstatblk, int nstatblks,
+                 int nsum, float* sk, void* stream);
+
 /* Channel-major -> time-major copy (the SIGPROC .nohead.fil layout,
  * PIPE:777). */
 int vfrb_fb_to_time_major(const float* src_cm, int64_t chan_stride, int64_t row0, uint32_t row_mask,
@@ -290,6 +301,13 @@ int vfrb_fb_to_time_major(const float* src_cm, int64_t chan_stride, int64_t row0
 #define VFRB_OUT_CHANSTATS 8       /* per-channel statistics (STATS)        */
 #define VFRB_OUT_FB 16             /* bandpass-subtracted FB, time-major    */
 #define VFRB_OUT_CANDS 32          /* candidate list                        */
+#define VFRB_OUT_FLAGS 64          /* per-row data flags (VFRB_ROW_*)       */
+
+/* Row flags: an FB row is flagged when any frame whose samples it holds (in
+ * either pol) carried the VDIF invalid bit (the reference ignores the bit,
+ * so the data are processed as usual), or was a zero-filled missing frame. */
+#define VFRB_ROW_INVALID 1
+#define VFRB_ROW_FILL 2
 
 typedef struct vfrb_plan vfrb_plan;
 
@@ -379,6 +397,12 @@ typedef struct vfrb_result {
   const float* box_snr;            /* [ndm] best boxcar SNR, or NULL          */
   const int32_t* box_start;        /* [ndm] its start (row0-relative)         */
   const int32_t* box_width;        /* [ndm] its width in samples              */
+  const float* chan_sk;            /* [nstatblks][nchan] spectral kurtosis of
+                                    * the raw FB (with chan_ave), or NULL   */
+  int64_t nflag_rows;
+  const uint8_t* row_flags;        /* VFRB_OUT_FLAGS: VFRB_ROW_* per FB row;
+                                    * block mode: block rows [0, MAXNT);
+                                    * stream mode: rows [row0, row0 + nt)   */
 } vfrb_result;
 
 int vfrb_plan_create(vfrb_plan** plan, const vfrb_params* params);

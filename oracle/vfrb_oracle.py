@@ -141,6 +141,13 @@ class RefPairReader:
         self.npartleft = 0
         self.flag_eof = 1
         self.log: list[str] = []
+        # row-flag bookkeeping (new-build extension; the reference ignores the
+        # invalid bit): flag of the payload in data[p] / tmp[p] (1 = its
+        # header had the invalid bit, 2 = zero fill), and per pair made
+        # current (pair k = pol bytes [5000k, 5000(k+1))) the OR of both pols
+        self.dflag = [0, 0]
+        self.tflag = [0, 0]
+        self.pair_flags: list[int] = []
 
     # fread of a header then a payload (PIPE:829-883)
     def _raw_read(self, p) -> int:
@@ -156,6 +163,7 @@ class RefPairReader:
             return 1
         self.data[p] = bytes(self.buf[self.pos:self.pos + DATALEN])
         self.pos += DATALEN
+        self.dflag[p] = self.hdr[p]["invalid"]
         return 0
 
     def _checkframeskip(self, p):  # PIPE:888-930 / TS:895-937
@@ -167,6 +175,7 @@ class RefPairReader:
                 self.nskip[p] = fnum - self.expected[p] + (fsec - self.expsec[p]) * FRAMESPERSEC
                 self.tmp[p] = self.data[p]
                 self.data[p] = bytes(DATALEN)
+                self.tflag[p], self.dflag[p] = self.dflag[p], 2
                 self.log.append(f"skip{p} {self.nskip[p]}")
             self.expected[p] = (fnum + 1) % FRAMESPERSEC
             self.expsec[p] = fsec + (1 if self.expected[p] == 0 else 0)
@@ -178,6 +187,7 @@ class RefPairReader:
                 self.nskip[p] = n
                 self.tmp[p] = self.data[p]
                 self.data[p] = bytes(DATALEN)
+                self.tflag[p], self.dflag[p] = self.dflag[p], 2
                 self.log.append(f"skip{p} {n}")
             self.expected[p] = (fnum + 1) % FRAMESPERSEC
 
@@ -186,6 +196,7 @@ class RefPairReader:
             self.nskip[p] -= 1
             if self.nskip[p] == 0:
                 self.data[p] = self.tmp[p]
+                self.dflag[p] = self.tflag[p]
             return 0
         if self._raw_read(p):
             return 1
@@ -193,7 +204,10 @@ class RefPairReader:
         return 0
 
     def readtwoframe(self) -> int:  # PIPE:1031-1040
-        return self._readone(0) or self._readone(1)
+        st = self._readone(0) or self._readone(1)
+        if not st:
+            self.pair_flags.append(self.dflag[0] | self.dflag[1])
+        return st
 
     def init_dada(self) -> int:  # TS:767-826 (discard NFRAMEDADAINIT pairs)
         for _ in range(NFRAMEDADAINIT):
@@ -202,6 +216,7 @@ class RefPairReader:
         return 0
 
     def initframe01(self) -> int:  # PIPE:1058-1131, TS:1070-1145
+        self.pair_flags = []
         if self._raw_read(0):
             return 1
         if self.hdr[0]["threadid"] != 0:
@@ -227,6 +242,7 @@ class RefPairReader:
         for p in (0, 1):
             self.expected[p] = (self.hdr[p]["frame"] + 1) % FRAMESPERSEC
             self.expsec[p] = self.hdr[p]["seconds"] + (1 if self.expected[p] == 0 else 0)
+        self.pair_flags.append(self.dflag[0] | self.dflag[1])
         return 0
 
     def init_ts(self) -> int:
@@ -285,6 +301,33 @@ def read_bundles(data, L: Layout, mode="pipe", max_bundles=None, dada_skip=False
             break
         out.append(b)
     return h0, out, r
+
+
+def row_flags(pair_flags, L: Layout, nrows: int) -> np.ndarray:
+    """Flags of FB rows 0 .. nrows-1 (new-build extension): row r holds pol
+    bytes [r*S, (r+1)*S), S = NAVE*TWONCHAN, i.e. pairs r*S//5000 ..
+    ((r+1)*S-1)//5000; its flag is the OR of theirs (1 = a frame with the
+    VDIF invalid bit, 2 = a zero-filled missing frame)."""
+    pf = np.asarray(pair_flags, np.uint8)
+    S = L.nave * L.twonchan
+    out = np.zeros(nrows, np.uint8)
+    for r in range(nrows):
+        out[r] = np.bitwise_or.reduce(pf[r * S // DATALEN:((r + 1) * S - 1) // DATALEN + 1])
+    return out
+
+
+def block_rows(L: Layout, max_delay: int, q: int) -> np.ndarray:
+    """Absolute FB row of each row of block q (parity-block mode): block 0 is
+    rows 0 .. MAXNT-1; a later block starts with the previous block's last
+    max_delay rows, and its rows from first = (max_delay//NBUNDLE)*NBUNDLE
+    on (where the refill starts, overwriting carried rows) follow the
+    previous block's last row."""
+    i = np.arange(L.maxnt, dtype=np.int64)
+    if q == 0:
+        return i
+    first = (max_delay // L.nbundle) * L.nbundle
+    end = L.maxnt + (q - 1) * (L.maxnt - first)  # absolute row after the previous block
+    return np.where(i < first, end - max_delay + i, end - first + i)
 
 
 # --- a5-a9: channeliser (PIPE:574-632, 1292-1322) ---------------------------
@@ -517,6 +560,24 @@ def cluster_cands(cands, dm_tol: int, t_tol: int):
     label_of_root = {root: k for k, (root, _) in enumerate(reps)}
     labels = [label_of_root[find(i)] for i in range(n)]
     return [cands[b] for _, b in reps], labels
+
+
+def chan_sk(fb_raw: np.ndarray, ncolstatblk: int, nstatblks: int, nsum: int) -> np.ndarray:
+    """Spectral kurtosis (new-build extension; the reference has none) per
+    (stat block, channel) of the RAW FB (before bandpass subtraction): the
+    generalised estimator of Nita & Gary (2010),
+    SK = (M*nsum + 1)/(M - 1) * (M*S2/S1^2 - 1), M rows, S1 = sum x,
+    S2 = sum x^2, nsum = raw power values per FB sample (2 pols x NAVE)."""
+    x = np.asarray(fb_raw, np.float64)
+    maxnt, nch = x.shape
+    out = np.zeros((nstatblks, nch))
+    for k in range(nstatblks):
+        blk = x[ncolstatblk * k:min(ncolstatblk * (k + 1), maxnt)]
+        m = blk.shape[0]
+        s1 = blk.sum(axis=0)
+        s2 = (blk * blk).sum(axis=0)
+        out[k] = (m * nsum + 1.0) / (m - 1.0) * (m * s2 / (s1 * s1) - 1.0)
+    return out
 
 
 # --- a16: calcstats per channel (STATS:910-946) -----------------------------

@@ -152,9 +152,10 @@ def test_block_mode_stats_chain(vf, O, co):
         assert np.array_equal(r["chan_outlier"], o)
 
 
-def _stream_run(vf, dms, bufs, storage=0, chunk=0.25, splits=None, order=None, **kw):
+def _stream_run(vf, dms, bufs, storage=0, chunk=0.25, splits=None, order=None, outputs=None, **kw):
+    outputs = outputs if outputs is not None else vf.OUT_DEDISP | vf.OUT_DMSTATS | vf.OUT_CANDS
     plan = vf.Plan(dms, nave=2, muoslowfreq=384.0, mode=vf.MODE_STREAM, storage=storage, chunk_seconds=chunk,
-                   nstreams=len(bufs), outputs=vf.OUT_DEDISP | vf.OUT_DMSTATS | vf.OUT_CANDS, **kw)
+                   nstreams=len(bufs), outputs=outputs, **kw)
     rng = np.random.default_rng(0)
     pos = [0] * len(bufs)
     live = list(range(len(bufs)))
@@ -171,6 +172,72 @@ def _stream_run(vf, dms, bufs, storage=0, chunk=0.25, splits=None, order=None, *
     for r in res:
         per.setdefault(r["stream"], []).append(r)
     return plan, per
+
+
+def _rfi_vdif(duration, seed, drop=()):
+    """RFI-heavy stream (tones, bursts, 10% invalid-flagged frames) with the
+    listed frame pairs removed (gaps the reader zero-fills)."""
+    from vlite_frb_b200 import synth
+    fr = synth.make_vdif(synth.StreamSpec(duration=duration, seed=seed, rfi=synth.Rfi())).numpy()
+    fr = fr.reshape(-1, 2, 5032)
+    return np.ascontiguousarray(np.delete(fr, list(drop), axis=0)).reshape(-1)
+
+
+def _pair_flags(O, buf, L, mode="pipe"):
+    _, _, r = O.read_bundles(buf, L, mode=mode)
+    return r.pair_flags
+
+
+def test_stats_rfi_sk_and_row_flags(vf, O, co):
+    """RFI-heavy STATS block mode: spectral kurtosis of the raw block per
+    (channel, TIMESTATS block) within 1e-3 of the FP64 oracle; row flags
+    (invalid bit, zero fill) identical to the oracle's."""
+    nave, maxtime, tstat = 4, 0.5, 0.1
+    buf = _rfi_vdif(1.3, seed=7, drop=(9000, 9001, 20000))
+    plan = vf.Plan(None, nave=nave, maxtime=maxtime, timestats=tstat, mode=vf.MODE_BLOCK,
+                   outputs=vf.OUT_CHANSTATS | vf.OUT_FLAGS)
+    plan.push(0, buf)
+    plan.push(0, None)
+    res = plan.drain()
+    L = O.Layout(nave=nave, maxtime=maxtime)
+    rows = _oracle_rows(O, co, buf, L)
+    ncol = int(tstat / L.tchan)
+    nblk = int(np.float32(maxtime) / np.float32(tstat))
+    blocks = list(O.run_stats_blocks(rows, L))
+    flags = O.row_flags(_pair_flags(O, buf, L), L, len(blocks) * L.maxnt)
+    assert len(res) == len(blocks) == 2
+    assert flags.any() and (flags & 2).any()
+    for r, (q, fb) in zip(res, blocks):
+        sk = O.chan_sk(fb, ncol, nblk, 2 * nave)
+        e = np.max(np.abs(r["chan_sk"] - sk))
+        print(f"block {q}: SK max abs err {e:.2e}, SK range {sk.min():.3f} .. {sk.max():.3f}")
+        assert e <= 1e-3
+        assert np.array_equal(r["row_flags"], flags[q * L.maxnt:(q + 1) * L.maxnt])
+
+
+def test_pipe_block_and_stream_row_flags(vf, O, co):
+    """Row flags in parity-block mode with the overlap carry (each block row
+    maps to its absolute row) and in stream mode (rows [row0, row0 + nt) of
+    each chunk), identical to the oracle's."""
+    nave, maxtime = 2, 0.8
+    dms = np.arange(0, 10.5, 0.5, dtype=np.float32)
+    buf = _rfi_vdif(2.0, seed=8, drop=(15000, 30001))
+    plan = vf.Plan(dms, nave=nave, muoslowfreq=384.0, maxtime=maxtime, mode=vf.MODE_BLOCK,
+                   outputs=vf.OUT_DEDISP | vf.OUT_FLAGS)
+    plan.push(0, buf)
+    plan.push(0, None)
+    res = plan.drain()
+    L = O.Layout(nave=nave, muoslowfreq=384.0, maxtime=maxtime)
+    off, md = O.delay_table(dms, L.fch1, L.chanbw, L.tchan, L.nchanout)
+    pf = _pair_flags(O, buf, L)
+    flags = O.row_flags(pf, L, len(pf) * 5000 // (nave * 12500))
+    assert len(res) == 2
+    for q, r in enumerate(res):
+        assert np.array_equal(r["row_flags"], flags[O.block_rows(L, md, q)])
+    plan, per = _stream_run(vf, dms, [buf], outputs=vf.OUT_DEDISP | vf.OUT_FLAGS)
+    got = np.concatenate([r["row_flags"] for r in per[0]])
+    assert per[0][0]["row0"] == 0 and got.size > L.maxnt
+    assert np.array_equal(got, flags[:got.size]) and (got & 2).any() and (got & 1).any()
 
 
 def test_stream_mode_matches_oracle(vf, O, co):

@@ -252,6 +252,24 @@ def test_bandpass_copy_mode(vf):
         vf.bandpass(torch.from_numpy(x).to(dev), subtract_mode=2)
 
 
+def test_chan_sk_matches_oracle(vf, O):
+    """Spectral kurtosis of a raw time-major FB against the FP64 oracle (FP64
+    sums of the same FP32 values: within FP32 output rounding)."""
+    torch = _torch()
+    rng = np.random.default_rng(12)
+    nsum, ncol, nblk, nch = 8, 300, 4, 333
+    rows = ncol * nblk - 70  # short last block
+    x = (rng.gamma(nsum, 1.0 / nsum, (rows, nch)) * rng.uniform(50, 500, nch)).astype(np.float32)
+    x[:, 7] = 3.0
+    x[100:104, 9] *= 30
+    got = vf.chan_sk(torch.from_numpy(x).cuda(), ncol, nblk, nsum).cpu().numpy()
+    ref = O.chan_sk(x.astype(np.float64), ncol, nblk, nsum)
+    assert np.max(np.abs(got - ref)) <= 1e-5 * max(1.0, np.abs(ref).max())
+    assert abs(got[:, 7]).max() < 1e-5 and got[0, 9] > 3
+    with pytest.raises(RuntimeError):  # an empty last block
+        vf.chan_sk(torch.from_numpy(x).cuda(), ncol, nblk, nsum, nrows=ncol * (nblk - 1))
+
+
 def _dd_case(ndm=40, nch=256, nt=1000, seed=2, dm_max=30.0, irregular=False):
     rng = np.random.default_rng(seed)
     fch1, chanbw, tchan = 384.0, 0.25, 0.001

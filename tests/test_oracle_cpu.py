@@ -107,3 +107,64 @@ def test_rfi_modes_oracle_matches_loops(O):
     z = O.subtract_zero(fb)
     assert np.allclose(z, _loop_subtract_zero(fb), rtol=0, atol=1e-12)
     assert np.array_equal(z[11], fb[11])  # sig 0: nothing inside the open interval, mean 0 subtracted
+
+
+def _frames_np(duration, seed=0, rfi=None):
+    from vlite_frb_b200 import synth
+    spec = synth.StreamSpec(duration=duration, seed=seed, rfi=rfi)
+    return synth.make_vdif(spec).numpy().reshape(-1, 2, 5032).copy()
+
+
+def test_row_flags_known_answer(vf, O):
+    """Pair flags from the reader restatement, pinned by hand: the invalid bit
+    of either pol flags its pair (1); a missing pair becomes zero fill (2) and
+    the frame that revealed the gap is used one pair later with its own bit."""
+    fr = _frames_np(0.02)                      # 512 pairs, frames 0..511
+    fr[7, 1, 3] |= 0x80                        # pol 1 of pair 7: invalid bit
+    fr[30, 0, 3] |= 0x80                       # pol 0 of pair 30
+    fr = np.delete(fr, 20, axis=0)             # pair 20 missing: frame 21 reveals the gap
+    fr[20, 0, 3] |= 0x80                       # ... and frame 21 (now at index 20) is invalid on pol 0
+    r = O.RefPairReader(fr.reshape(-1))
+    assert r.initframe01() == 0
+    while not r.readtwoframe():
+        pass
+    pf = np.array(r.pair_flags)
+    want = np.zeros(512, np.uint8)
+    want[7] = 1
+    want[20] = 2          # the fill pair
+    want[21] = 1          # frame 21, invalid, used after the fill
+    want[30] = 1
+    assert len(pf) == 512 and np.array_equal(pf, want)  # 511 pairs read + the fill pair
+    L = O.Layout(nave=1, muoslowfreq=384.0)    # S = 12500 bytes = 2.5 pairs per row
+    rf = O.row_flags(pf, L, 200)
+    # pair 7 (bytes 35000-39999) straddles rows 2 and 3; pairs 20-21 lie in
+    # row 8, pair 30 in row 12
+    assert list(np.nonzero(rf)[0]) == [2, 3, 8, 12]
+    assert rf[8] == 3 and rf[2] == rf[3] == rf[12] == 1
+
+
+def test_block_rows_map(O):
+    L = O.Layout(nave=2, muoslowfreq=384.0, maxtime=0.8)   # MAXNT 4096, NBUNDLE 32
+    md = 100                                               # first = 96
+    b1 = O.block_rows(L, md, 1)
+    assert b1[0] == L.maxnt - md and b1[95] == L.maxnt - md + 95
+    assert b1[96] == L.maxnt and b1[-1] == 2 * L.maxnt - 96 - 1
+    b2 = O.block_rows(L, md, 2)
+    assert b2[96] == b1[-1] + 1 and b2[0] == b1[-1] + 1 - md
+
+
+def test_chan_sk_gaussian_expectation(O):
+    """SK of Gamma(nsum) power (Gaussian-noise detection statistics) is 1 in
+    expectation; a steady tone (constant power) drives it to 0, a burst far
+    above 1."""
+    rng = np.random.default_rng(3)
+    nsum, m, nblk = 8, 1024, 6
+    x = rng.gamma(nsum, 1.0 / nsum, (m * nblk, 64)) * 50.0
+    x[:, 10] = 50.0                                   # constant: S2 = S1^2/M
+    x[5:9, 20] *= 40.0                                # burst in block 0
+    sk = O.chan_sk(x, m, nblk, nsum)
+    ok = np.ones(64, bool)
+    ok[[10, 20]] = False
+    assert abs(sk[:, ok].mean() - 1.0) < 0.01
+    assert np.allclose(sk[:, 10], 0.0, atol=1e-9)
+    assert sk[0, 20] > 5 and abs(sk[1, 20] - 1) < 0.2

@@ -223,3 +223,49 @@ def test_timeseries_tool_outputs(vf, O, co, tmp_path):
             assert inf == O.presto_inf(os.path.basename(base), O.vdif_dmjd(h0), a.size, tsamp, dms[d],
                                        320.0 + 0.5 * L.chanbw, L.nchanout * L.chanbw, L.nchanout, L.chanbw)
     assert glob.glob(str(tmp_path / "ts_*.log"))
+
+
+def test_stats_and_timeseries_sk_and_flags(vf, O, co, tmp_path):
+    """RFI-heavy input (tones, bursts, 10% invalid-flagged frames, two missing
+    pairs): vdifDADA2stats -sk -flags writes per block the spectral kurtosis
+    of the raw filterbank and the row flags; vdifDADA2timeseries -flags writes
+    one flag byte per series sample.  SK within 1e-3 of the FP64 oracle,
+    flags identical."""
+    from vlite_frb_b200 import synth
+    fr = synth.make_vdif(synth.StreamSpec(duration=3.2, seed=13, rfi=synth.Rfi())).numpy().reshape(-1, 2, 5032)
+    buf = np.ascontiguousarray(np.delete(fr, [12345, 40000], axis=0)).reshape(-1)
+    buf.tofile(tmp_path / "in.vdif")
+    nave, maxtime, tstat = 4, 0.5, 0.1
+    r = subprocess.run([_tool("vdifDADA2stats"), "-i", "in.vdif", "-o", "f", "-maxtime", str(maxtime), "-timestats",
+                        str(tstat), "-sk", "-flags"], cwd=tmp_path, capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, (r.stderr, (tmp_path / "f.log").read_text())
+    L = O.Layout(nave=nave, maxtime=maxtime)
+    _, bundles, rd = O.read_bundles(buf, L)
+    rows = co.channelise(np.concatenate([b[0] for b in bundles]), np.concatenate([b[1] for b in bundles]), L)
+    ncol = int(tstat / L.tchan)
+    nblk = int(np.float32(maxtime) / np.float32(tstat))
+    blocks = list(O.run_stats_blocks(rows, L))
+    sk = np.fromfile(tmp_path / "f.sk", np.float32).reshape(-1, nblk, L.nchanout)
+    fl = np.fromfile(tmp_path / "f.flags", np.uint8).reshape(-1, L.maxnt)
+    flags = O.row_flags(rd.pair_flags, L, len(blocks) * L.maxnt)
+    assert sk.shape[0] == fl.shape[0] == len(blocks) >= 5
+    for q, fb in blocks:
+        assert np.max(np.abs(sk[q] - O.chan_sk(fb, ncol, nblk, 2 * nave))) <= 1e-3
+        assert np.array_equal(fl[q], flags[q * L.maxnt:(q + 1) * L.maxnt])
+    assert (flags & 1).any() and (flags & 2).any()
+    # timeseries: 3840 channels, blocks with the max-delay carry
+    maxtime = 1.5
+    r = subprocess.run([_tool("vdifDADA2timeseries"), "-d", "-i", "in.vdif", "-o", "ts", "-noskip", "-maxtime",
+                        str(maxtime), "-flags"], cwd=tmp_path, capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr
+    dms = np.array([0.0, 119.3], np.float32)
+    L = O.Layout(nave=nave, nchanout_fixed=3840, maxtime=maxtime)
+    off, md = O.delay_table(dms, L.fch1, L.chanbw, L.tchan, L.nchanout)
+    _, bundles, rd = O.read_bundles(buf, L, mode="ts")
+    nrows = len(bundles) * L.nbundle
+    nblocks = len(list(O.run_blocks(np.zeros((nrows, 1)), L, md)))
+    flags = O.row_flags(rd.pair_flags, L, nrows + L.maxnt)
+    nt = L.maxnt - md
+    want = np.concatenate([flags[O.block_rows(L, md, q)][:nt] for q in range(nblocks)])
+    got = np.fromfile(tmp_path / "ts.flags", np.uint8)
+    assert nblocks >= 1 and np.array_equal(got, want)

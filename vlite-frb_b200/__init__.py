@@ -111,6 +111,8 @@ _lib.vfrb_dedisperse_workspace_bytes.argtypes = [C.c_void_p, C.c_int64]
 _lib.vfrb_dedisperse.argtypes = [C.c_void_p, C.POINTER(DdArgs), C.c_void_p]
 _lib.vfrb_fb_to_time_major.argtypes = [C.c_void_p, C.c_int64, C.c_int64, C.c_uint32, C.c_int, C.c_int, C.c_void_p,
                                        C.c_int64, C.c_void_p]
+_lib.vfrb_chan_sk.argtypes = [C.c_void_p, C.c_int64, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_void_p,
+                               C.c_void_p]
 for _n in ("vfrb_subtract_bp_full", "vfrb_subtract_zero"):
     getattr(_lib, _n).argtypes = [C.c_void_p, C.c_int64, C.c_int64, C.c_uint32, C.c_int, C.c_int64, C.c_void_p]
 
@@ -203,6 +205,19 @@ def bandpass(fb_tm, nrows=None, storage=F32, out=None, out_row0=0, out_row_mask=
                tm_out=_ptr(tm_out), tm_row_stride=tm_out.stride(0) if tm_out is not None else 0,
                d_err=_ptr(d_err), subtract_mode=subtract_mode)
     _check(_lib.vfrb_bandpass(C.byref(a), _stream(stream)), "vfrb_bandpass")
+    return out
+
+
+def chan_sk(fb_tm, ncolstatblk, nstatblks, nsum, nrows=None, out=None, stream=None):
+    """Spectral kurtosis per (channel, block of ncolstatblk rows) of a raw
+    time-major FP32 FB (vfrb_chan_sk); returns [nstatblks][nchan] float32."""
+    torch = _torch()
+    nrows = fb_tm.shape[0] if nrows is None else nrows
+    nchan = fb_tm.shape[1]
+    if out is None:
+        out = torch.empty((nstatblks, nchan), dtype=torch.float32, device=fb_tm.device)
+    _check(_lib.vfrb_chan_sk(fb_tm.data_ptr(), fb_tm.stride(0), nchan, nrows, ncolstatblk, nstatblks, nsum,
+                             out.data_ptr(), _stream(stream)), "vfrb_chan_sk")
     return out
 
 
@@ -331,7 +346,8 @@ def fb_to_time_major(fb_cm, nrows=None, row0=0, row_mask=0xFFFFFFFF, out=None, s
 # ---- plan / stream API -------------------------------------------------------------
 MODE_BLOCK, MODE_STREAM = 0, 1
 READER_PIPE, READER_TS = 0, 1
-OUT_DEDISP, OUT_DMSTATS, OUT_SIGMA, OUT_CHANSTATS, OUT_FB, OUT_CANDS = 1, 2, 4, 8, 16, 32
+OUT_DEDISP, OUT_DMSTATS, OUT_SIGMA, OUT_CHANSTATS, OUT_FB, OUT_CANDS, OUT_FLAGS = 1, 2, 4, 8, 16, 32, 64
+ROW_INVALID, ROW_FILL = 1, 2
 BP_CAL, BP_FULL = 0, 1
 VFRB_PENDING = 9
 
@@ -360,7 +376,8 @@ class Result(C.Structure):
                 ("nstatblks", C.c_int32), ("chan_ave", C.c_void_p), ("chan_sig", C.c_void_p),
                 ("chan_outlier", C.c_void_p), ("ncand", C.c_int32), ("cands", C.c_void_p),
                 ("latency_ms", C.c_double), ("device_errors", C.c_int32), ("box_snr", C.c_void_p),
-                ("box_start", C.c_void_p), ("box_width", C.c_void_p)]
+                ("box_start", C.c_void_p), ("box_width", C.c_void_p), ("chan_sk", C.c_void_p),
+                ("nflag_rows", C.c_int64), ("row_flags", C.c_void_p)]
 
 
 _lib.vfrb_cluster_cands.argtypes = [C.POINTER(Cand), C.c_int32, C.c_int32, C.c_int64, C.POINTER(Cand),
@@ -464,9 +481,10 @@ class Plan:
             out[k] = _arr(getattr(r, k), ndm, dt)
         fb = _arr(r.fb, r.fb_rows * nch, C.c_float)
         out["fb"] = fb.reshape(r.fb_rows, nch) if fb is not None else None
-        for k in ("chan_ave", "chan_sig", "chan_outlier"):
+        for k in ("chan_ave", "chan_sig", "chan_outlier", "chan_sk"):
             a = _arr(getattr(r, k), r.nstatblks * nch, C.c_float)
             out[k] = a.reshape(r.nstatblks, nch) if a is not None else None
+        out["row_flags"] = _arr(r.row_flags, r.nflag_rows, C.c_uint8)
         cands = []
         if r.ncand and r.cands:
             ca = C.cast(r.cands, C.POINTER(Cand))

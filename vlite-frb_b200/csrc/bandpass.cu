@@ -198,6 +198,45 @@ int launch_chan_stats(const vfrb_cs_args& a, cudaStream_t s) {
   return cuda_status(cudaGetLastError());
 }
 
+// ---- spectral kurtosis per (channel, statistics block) ----------------------
+// Generalised SK estimator (Nita & Gary 2010) of the raw (not bandpass-
+// subtracted) power: with M rows in the block, S1 = sum x, S2 = sum x^2 and
+// nsum = N*d raw power values per FB sample (2 pols x NAVE spectra, each an
+// exponential variable for Gaussian noise),
+//   SK = (M*nsum + 1)/(M - 1) * (M*S2/S1^2 - 1),
+// whose expectation is 1 for Gaussian noise; narrowband RFI drives it below 1
+// (steady tones) or far above it (bursts); a one-row block gives inf/NaN as
+// M - 1 = 0.  FP64 sums.  The FB is time-major,
+// so a warp reads 32 consecutive channels of a row: 128-byte segments.
+__global__ void __launch_bounds__(256) k_chan_sk(const float* __restrict__ fb, long long row_stride, int nchan,
+                                                 int nrows, int ncolstatblk, int nstatblks, double nsum,
+                                                 float* __restrict__ sk) {
+  const int c = blockIdx.x * 256 + threadIdx.x;
+  const int k = blockIdx.y;
+  if (c >= nchan || k >= nstatblks) return;
+  const long long r0 = (long long)ncolstatblk * k;
+  const long long r1 = min(r0 + ncolstatblk, (long long)nrows);
+  double s1 = 0.0, s2 = 0.0;
+  for (long long r = r0; r < r1; ++r) {
+    const double x = (double)fb[r * row_stride + c];
+    s1 += x;
+    s2 += x * x;
+  }
+  const double m = (double)(r1 - r0);
+  const double v = (m * nsum + 1.0) / (m - 1.0) * (m * s2 / (s1 * s1) - 1.0);
+  sk[(long long)k * nchan + c] = (float)v;
+}
+
+int launch_chan_sk(const float* fb_tm, long long row_stride, int nchan, int nrows, int ncolstatblk, int nstatblks,
+                   int nsum, float* sk, cudaStream_t s) {
+  if (!fb_tm || !sk || nchan <= 0 || nstatblks <= 0 || ncolstatblk <= 1 || nsum < 1 || row_stride < nchan ||
+      (long long)nrows - (long long)ncolstatblk * (nstatblks - 1) < 1 || nstatblks > 65535)
+    return VFRB_ERR_ARG;
+  dim3 grid((unsigned)((nchan + 255) / 256), (unsigned)nstatblks);
+  k_chan_sk<<<grid, 256, 0, s>>>(fb_tm, row_stride, nchan, nrows, ncolstatblk, nstatblks, (double)nsum, sk);
+  return cuda_status(cudaGetLastError());
+}
+
 // ---- channel-major -> time-major copy ---------------------------------------
 __global__ void __launch_bounds__(256) k_transpose(const float* __restrict__ src, long long chan_stride,
                                                    unsigned row_mask, long long row0, int nchan, int nrows,

@@ -108,8 +108,9 @@ struct ResultSlot {
   int32_t *frb = nullptr, *arg = nullptr, *err = nullptr;
   float* bsnr = nullptr;  // boxcar search: best SNR, start, width per trial
   int32_t *bt = nullptr, *bw = nullptr;
-  float *cave = nullptr, *csig = nullptr, *cout = nullptr;
+  float *cave = nullptr, *csig = nullptr, *cout = nullptr, *csk = nullptr;
   std::vector<vfrb_cand> cands;
+  std::vector<uint8_t> flags;  // VFRB_ROW_* of the result's rows
   cudaEvent_t ev = nullptr;
   double t_data = 0.0;
   volatile double t_done = 0.0;
@@ -152,6 +153,10 @@ struct StreamSt {
   int sb_i = 0;
   int64_t slots_cap = 0;
   std::vector<int64_t> e0, e1;  // pair entries: frame index, -1 fill, <= -2 stash slot
+  std::vector<uint8_t> finv;    // VDIF invalid bit of each ring frame slot
+  uint8_t stash_flag[kStash] = {};
+  std::vector<uint8_t> rflags;  // VFRB_ROW_* per FB row: block rows, or a ring of rows (stream)
+  int64_t fmask = 0;
   size_t ehead = 0;             // consumed entries at the front of e0/e1
   int64_t ebase = 0;            // global index of e0[ehead]
   bool ended = false;
@@ -185,7 +190,7 @@ struct StreamSt {
   int32_t *d_bt = nullptr, *d_bw = nullptr;
   void* d_ws = nullptr;
   size_t ws_bytes = 0;
-  float *d_cave = nullptr, *d_csig = nullptr, *d_cout = nullptr, *d_fbt = nullptr;
+  float *d_cave = nullptr, *d_csig = nullptr, *d_cout = nullptr, *d_csk = nullptr, *d_fbt = nullptr;
   int64_t out_stride = 0;
   std::vector<std::unique_ptr<ResultSlot>> slots;
 };
@@ -320,6 +325,7 @@ int alloc_slot(vfrb_plan* pl, StreamSt* s, ResultSlot** out) {
     ST(hmalloc(pl, &r->cave, (size_t)pl->nstatblks * nch * 4));
     ST(hmalloc(pl, &r->csig, (size_t)pl->nstatblks * nch * 4));
     ST(hmalloc(pl, &r->cout, (size_t)pl->nstatblks * nch * 4));
+    ST(hmalloc(pl, &r->csk, (size_t)pl->nstatblks * nch * 4));
   }
   ST(hmalloc(pl, &r->err, 4));
   ST(mkevent(pl, &r->ev));
@@ -333,6 +339,13 @@ inline int64_t entry_offset(const StreamSt* s, int64_t v) {
   if (v >= 0) return (v % s->ring_frames) * kFrameLen + kHdrLen;
   if (v == -1) return -1;
   return s->ring_frames * kFrameLen + (-2 - v) * (int64_t)kDataLen;
+}
+
+// VFRB_ROW_* contribution of one pol's entry
+inline uint8_t entry_flag(const StreamSt* s, int64_t v) {
+  if (v >= 0) return s->finv[(size_t)(v % s->ring_frames)];
+  if (v == -1) return VFRB_ROW_FILL;
+  return s->stash_flag[-2 - v];
 }
 
 int64_t npairs(const StreamSt* s) { return s->ebase + (int64_t)(s->e0.size() - s->ehead); }
@@ -371,6 +384,19 @@ int launch_rows(vfrb_plan* pl, StreamSt* s, int64_t row_first, int64_t nrows, fl
     const size_t k = s->ehead + (size_t)(e_lo - s->ebase + i);
     b.h[i] = entry_offset(s, s->e0[k]);
     b.h[s->slots_cap + i] = entry_offset(s, s->e1[k]);
+  }
+  if (want(pl, VFRB_OUT_FLAGS)) {
+    // row r holds pol bytes [r*S, (r+1)*S): the entries that cover them
+    const bool blk = pl->P.mode == VFRB_MODE_BLOCK;
+    for (int64_t r = 0; r < nrows; ++r) {
+      const int64_t a0 = (row_first + r) * S / kDataLen, a1 = ((row_first + r + 1) * S - 1) / kDataLen;
+      uint8_t f = 0;
+      for (int64_t e = a0; e <= a1; ++e) {
+        const size_t k = s->ehead + (size_t)(e - s->ebase);
+        f |= entry_flag(s, s->e0[k]) | entry_flag(s, s->e1[k]);
+      }
+      s->rflags[(size_t)(blk ? out_row0 + r : (row_first + r) & s->fmask)] = f;
+    }
   }
   // The upload goes on the copy stream: host-to-device copies queued on the
   // compute stream would sit in the copy engine's queue until the compute
@@ -535,6 +561,16 @@ int emit(vfrb_plan* pl, StreamSt* s, int64_t seq, int64_t row0, int64_t nt, bool
     CK(cudaMemcpyAsync(r->cave, s->d_cave, b, cudaMemcpyDeviceToHost, s->cs));
     CK(cudaMemcpyAsync(r->csig, s->d_csig, b, cudaMemcpyDeviceToHost, s->cs));
     CK(cudaMemcpyAsync(r->cout, s->d_cout, b, cudaMemcpyDeviceToHost, s->cs));
+    CK(cudaMemcpyAsync(r->csk, s->d_csk, b, cudaMemcpyDeviceToHost, s->cs));
+  }
+  r->flags.clear();
+  if (want(pl, VFRB_OUT_FLAGS)) {
+    if (pl->P.mode == VFRB_MODE_BLOCK) {
+      r->flags = s->rflags;
+    } else {
+      r->flags.resize((size_t)nt);
+      for (int64_t i = 0; i < nt; ++i) r->flags[(size_t)i] = s->rflags[(size_t)((row0 + i) & s->fmask)];
+    }
   }
   CK(cudaMemcpyAsync(r->err, s->d_err, 4, cudaMemcpyDeviceToHost, s->cs));
   CK(cudaMemsetAsync(s->d_err, 0, 4, s->cs));
@@ -567,6 +603,9 @@ int emit(vfrb_plan* pl, StreamSt* s, int64_t seq, int64_t row0, int64_t nt, bool
   o.chan_ave = cst ? r->cave : nullptr;
   o.chan_sig = cst ? r->csig : nullptr;
   o.chan_outlier = cst ? r->cout : nullptr;
+  o.chan_sk = cst ? r->csk : nullptr;
+  o.nflag_rows = (int64_t)r->flags.size();
+  o.row_flags = r->flags.empty() ? nullptr : r->flags.data();
   r->t_data = s->t_push;
   r->state = 1;
   pl->queue.push_back(r);
@@ -605,6 +644,9 @@ int block_complete(vfrb_plan* pl, StreamSt* s) {
     c.sig = s->d_csig;
     c.outlier = s->d_cout;
     ST(launch_chan_stats(c, s->cs));
+    // spectral kurtosis of the raw block (d_fb_tm is not modified by the bandpass)
+    ST(launch_chan_sk(s->d_fb_tm, nch, (int)nch, L.maxnt, pl->ncolstatblk, pl->nstatblks, 2 * L.nave, s->d_csk,
+                      s->cs));
   }
   if (pl->want_dd) ST(run_dedisp(pl, s, 0, L.maxnt, pl->nt_block, true));
   // absolute FB row of block row 0: block 0 starts at row 0; each later block
@@ -616,6 +658,7 @@ int block_complete(vfrb_plan* pl, StreamSt* s) {
   ST(emit(pl, s, s->blocks, row0, pl->want_dd ? pl->nt_block : 0, with_fb));
   if (pl->want_dd && pl->max_delay > 0) {
     CK(cudaMemcpyAsync(s->d_fb_tm, s->d_left, (size_t)pl->max_delay * nch * 4, cudaMemcpyDeviceToDevice, s->cs));
+    std::memmove(s->rflags.data(), s->rflags.data() + (L.maxnt - pl->max_delay), (size_t)pl->max_delay);
     s->loopcnt = pl->max_delay / L.nbundle;
   } else {
     s->loopcnt = 0;
@@ -787,6 +830,9 @@ int feed_frames(vfrb_plan* pl, StreamSt* s, const uint8_t* host, int64_t nf, boo
     }
     CK(cudaEventRecord(s->ev_copied, s->xs));
     CK(cudaStreamWaitEvent(s->cs, s->ev_copied, 0));
+    // the VDIF invalid bit (word 0, bit 31) of each frame, for row flags
+    for (int64_t f = 0; f < nb; ++f)
+      s->finv[(size_t)((s->frames_in + f) % s->ring_frames)] = (src[f * kFrameLen + 3] >> 7) & 1;
     // in-order pairs go straight to pair entries; the rest through the queue
     int64_t i = (int64_t)s->reader->run_fast(src, s->frames_in, (size_t)nb, s->e0, s->e1);
     for (; i < nb; ++i) {
@@ -833,6 +879,7 @@ int create_stream(vfrb_plan* pl, int id, int64_t ring_frames, int64_t R1, int64_
   for (auto& e : s->rel_ev) ST(mkevent(pl, &e));
   CK(cudaEventRecord(s->ev_consumed, s->cs));
   s->ring_frames = ring_frames;
+  s->finv.assign((size_t)ring_frames, 0);
   ST(dmalloc(pl, &s->d_frames, (size_t)ring_frames * kFrameLen + (size_t)kStash * kDataLen));
   s->stage_frames = (size_t)std::min<int64_t>(ring_frames / 4, 8192);
   for (int k = 0; k < kStageBufs; ++k) {
@@ -869,8 +916,10 @@ int create_stream(vfrb_plan* pl, int id, int64_t ring_frames, int64_t R1, int64_
       ST(dmalloc(pl, &s->d_cave, (size_t)pl->nstatblks * nch * 4));
       ST(dmalloc(pl, &s->d_csig, (size_t)pl->nstatblks * nch * 4));
       ST(dmalloc(pl, &s->d_cout, (size_t)pl->nstatblks * nch * 4));
+      ST(dmalloc(pl, &s->d_csk, (size_t)pl->nstatblks * nch * 4));
     }
     nt = pl->nt_block;
+    s->rflags.assign((size_t)L.maxnt, 0);
   } else {
     s->R1 = R1;
     ST(dmalloc(pl, &s->d_raw, (size_t)R1 * nch * 4));
@@ -879,6 +928,10 @@ int create_stream(vfrb_plan* pl, int id, int64_t ring_frames, int64_t R1, int64_
     ST(dmalloc(pl, &s->d_cm, (size_t)nch * R2 * sb));
     CK(cudaMemsetAsync(s->d_cm, 0, (size_t)nch * R2 * sb, s->cs));
     nt = pl->chunk_rows * pl->batch_chunks;
+    // rows from the oldest not yet emitted to the newest channelised: at
+    // most R2 (channel-major ring) + R1 (raw ring)
+    s->rflags.assign((size_t)(2 * std::max(R1, R2)), 0);
+    s->fmask = 2 * std::max(R1, R2) - 1;
   }
   if (pl->want_dd) {
     s->out_stride = nt;
@@ -903,6 +956,7 @@ int create_stream(vfrb_plan* pl, int id, int64_t ring_frames, int64_t R1, int64_
     if (v < 0) return v;
     const int k = sp->stash_next;
     sp->stash_next = (sp->stash_next + 1) % kStash;
+    sp->stash_flag[k] = sp->finv[(size_t)(v % sp->ring_frames)];
     const uint8_t* from = sp->d_frames + (v % sp->ring_frames) * kFrameLen + kHdrLen;
     uint8_t* to = sp->d_frames + sp->ring_frames * kFrameLen + (int64_t)k * kDataLen;
     if (cudaMemcpyAsync(to, from, kDataLen, cudaMemcpyDeviceToDevice, sp->cs) != cudaSuccess) {

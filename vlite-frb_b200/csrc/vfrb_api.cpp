@@ -171,6 +171,12 @@ int vfrb_chan_stats(const vfrb_cs_args* a, void* stream) {
   return vfrb::launch_chan_stats(*a, (cudaStream_t)stream);
 }
 
+int vfrb_chan_sk(const float* fb_tm, int64_t row_stride, int nchan, int nrows, int ncolstatblk, int nstatblks,
+                 int nsum, float* sk, void* stream) {
+  return vfrb::launch_chan_sk(fb_tm, row_stride, nchan, nrows, ncolstatblk, nstatblks, nsum, sk,
+                              (cudaStream_t)stream);
+}
+
 int vfrb_fb_to_time_major(const float* src_cm, int64_t chan_stride, int64_t row0, uint32_t row_mask, int nchan,
                           int nrows, float* dst_tm, int64_t dst_row_stride, void* stream) {
   return vfrb::launch_fb_transpose(src_cm, chan_stride, row_mask, row0, nchan, nrows, dst_tm, dst_row_stride,

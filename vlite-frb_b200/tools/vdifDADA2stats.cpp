@@ -13,7 +13,10 @@
 // Extensions: -k KEY (hex DADA key), -i FILE (read a VDIF file or "-"
 // instead of a ring), -o NAME (output base name), -maxtime S, -timestats S,
 // -nchan N / -nave N / -nb N (the reference fixes 6250 / 4 / 32),
-// -fullband (MUOSLOWFREQ 384).
+// -fullband (MUOSLOWFREQ 384), -sk (NAME.sk: per block the spectral kurtosis
+// of the raw filterbank, [NSTATBLKS][NCHANOUT] float32), -flags (NAME.flags:
+// per block one byte per row, bit 0 = a frame with the VDIF invalid bit,
+// bit 1 = a zero-filled missing frame).
 #include "tool_common.h"
 
 namespace {
@@ -31,7 +34,9 @@ void usage() {
                "\t  -maxtime (s)    block length (default 60)\n"
                "\t  -timestats (s)  statistics block (default 1)\n"
                "\t  -nchan/-nave/-nb (int)  channelisation (default 6250/4/32)\n"
-               "\t  -fullband       all 6250 channels (MUOSLOWFREQ 384)\n\n");
+               "\t  -fullband       all 6250 channels (MUOSLOWFREQ 384)\n"
+               "\t  -sk             write the spectral kurtosis per block to NAME.sk\n"
+               "\t  -flags          write the per-row data flags per block to NAME.flags\n\n");
 }
 
 }  // namespace
@@ -42,6 +47,7 @@ int main(int argc, char** argv) {
   std::string in, out = "vdifDADA2stats_";
   float maxtime = 60.f, timestats = 1.f;
   double muos = 360.0;
+  bool want_sk = false, want_flags = false;
   for (int i = 1; i < argc; ++i) {
     const bool more = i + 1 < argc;
     if (tool::eq(argv[i], "-h")) {
@@ -65,6 +71,10 @@ int main(int argc, char** argv) {
       nbundle = std::atoi(argv[++i]);
     } else if (tool::eq(argv[i], "-fullband")) {
       muos = 384.0;
+    } else if (tool::eq(argv[i], "-sk")) {
+      want_sk = true;
+    } else if (tool::eq(argv[i], "-flags")) {
+      want_flags = true;
     } else {
       std::fprintf(stderr, "Error! Unknown argument: %s\n\n", argv[i]);
       usage();
@@ -82,6 +92,12 @@ int main(int argc, char** argv) {
     std::fprintf(stderr, "Unable to open output STATS file: %s\n", statsname.c_str());
     return 2;
   }
+  FILE* skf = want_sk ? std::fopen((out + ".sk").c_str(), "wb") : nullptr;
+  FILE* flf = want_flags ? std::fopen((out + ".flags").c_str(), "wb") : nullptr;
+  if ((want_sk && !skf) || (want_flags && !flf)) {
+    std::fprintf(stderr, "Unable to open the output SK / flags file\n");
+    return 2;
+  }
   std::fprintf(log, "Running vdifDADA2stats (libvfrb, sm_100a)\n");
 
   vfrb_params p;
@@ -94,7 +110,7 @@ int main(int argc, char** argv) {
   p.timestats = timestats;
   p.mode = VFRB_MODE_BLOCK;
   p.reader = VFRB_READER_PIPE;
-  p.outputs = VFRB_OUT_CHANSTATS;
+  p.outputs = VFRB_OUT_CHANSTATS | (want_flags ? VFRB_OUT_FLAGS : 0);
   p.dms = nullptr;
   p.ndm = 0;
   vfrb_plan* plan = nullptr;
@@ -133,9 +149,13 @@ int main(int argc, char** argv) {
           tool::write_all(stats, r.chan_outlier, n * 4);
           std::fflush(stats);
         }
+        if (skf && r.chan_sk) tool::write_all(skf, r.chan_sk, n * 4);
+        if (flf && r.row_flags) tool::write_all(flf, r.row_flags, (size_t)r.nflag_rows);
         ++nblocks;
       });
   std::fclose(stats);
+  if (skf) std::fclose(skf);
+  if (flf) std::fclose(flf);
   vfrb_plan_destroy(plan);
   std::fprintf(log, "Processed %f [sec] of data\n", (double)nblocks * L.maxnt * L.tchan);
   std::fprintf(log, "\nfinished!\n");

@@ -13,7 +13,9 @@
 //
 // Extensions: -i FILE (read a VDIF file or "-" instead of the ring),
 // -noskip (do not skip the first 256000 frames), -maxtime S,
-// -infatend (also write the .inf headers of the files open at the end).
+// -infatend (also write the .inf headers of the files open at the end),
+// -flags (NAME.flags: one byte per time-series sample, appended with the
+// series, bit 0 = a frame with the VDIF invalid bit, bit 1 = zero fill).
 #include <ctime>
 
 #include "tool_common.h"
@@ -35,7 +37,8 @@ void usage() {
                "\t             -i (string)    read a VDIF file instead of the ring (- = stdin)\n"
                "\t             -noskip        do not skip the first 256000 frames per pol\n"
                "\t             -maxtime (s)   block length (default 30)\n"
-               "\t             -infatend      write .inf headers for the files open at the end\n\n"
+               "\t             -infatend      write .inf headers for the files open at the end\n"
+               "\t             -flags         write per-sample data flags to NAME.flags\n\n"
                "  DEFAULTS:\n"
                "\t             -k     dada\n"
                "\t             -o     testTIMESERIES\n"
@@ -98,7 +101,7 @@ int main(int argc, char** argv) {
   int twonchan = 0, nave = 0, nbundle = 0;
   unsigned key = 0xdada;
   std::string in, out;
-  bool skip = true, inf_at_end = false;
+  bool skip = true, inf_at_end = false, want_flags = false;
   float maxtime = 30.f;
   int i = 1;
   if (tool::eq(argv[i], "-d")) {
@@ -128,6 +131,8 @@ int main(int argc, char** argv) {
       maxtime = (float)std::atof(argv[++i]);
     } else if (tool::eq(argv[i], "-infatend")) {
       inf_at_end = true;
+    } else if (tool::eq(argv[i], "-flags")) {
+      want_flags = true;
     } else {
       std::fprintf(stderr, "Error! Unknown argument: %s\n\n", argv[i]);
       usage();
@@ -142,6 +147,7 @@ int main(int argc, char** argv) {
     return 2;
   }
   std::fprintf(log, "Running vdifDADA2timeseries (libvfrb, sm_100a)\n");
+  if (want_flags) std::remove((out + ".flags").c_str());
 
   const float dms[2] = {0.0f, 119.3f};  // 119.3 gives a 1-s sweep across the lower 39.3216 MHz (TS:437-438)
   vfrb_params p;
@@ -156,7 +162,7 @@ int main(int argc, char** argv) {
   p.mode = VFRB_MODE_BLOCK;
   p.reader = VFRB_READER_TS;
   p.dada_skip = skip ? 1 : 0;
-  p.outputs = VFRB_OUT_DEDISP | VFRB_OUT_SIGMA;
+  p.outputs = VFRB_OUT_DEDISP | VFRB_OUT_SIGMA | (want_flags ? VFRB_OUT_FLAGS : 0);
   vfrb_plan* plan = nullptr;
   int st = vfrb_plan_create(&plan, &p);
   if (st != VFRB_OK) {
@@ -220,6 +226,11 @@ int main(int argc, char** argv) {
                        append(base[d] + "_SIGMA.dat", r.dd_sigma + (size_t)d * r.nt, (size_t)r.nt);
           }
           ntimes += r.nt;
+          if (want_flags && r.row_flags && r.nflag_rows >= r.nt) {
+            FILE* ff = std::fopen((out + ".flags").c_str(), "ab");
+            files_ok = files_ok && ff && tool::write_all(ff, r.row_flags, (size_t)r.nt);
+            if (ff) std::fclose(ff);
+          }
         }
         if (utc_hour() == hrnext) {  // TS:696-739
           for (int d = 0; d < 2; ++d)
