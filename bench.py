@@ -123,7 +123,7 @@ class DevicePipeline:
     """K1 -> K2 -> K3 over the resident 60 s batch through the stage C ABI,
     with the overlap ring persisting across steps."""
 
-    def __init__(self, vf, frames, storage):
+    def __init__(self, vf, frames, storage, variant=0):
         import torch
         self.vf, self.torch = vf, torch
         self.storage = storage
@@ -162,6 +162,8 @@ class DevicePipeline:
             self.uscale = S
             self.inv = torch.full((nch,), 1.0 / S, device=dev)
         self.tune = self.plan.autotune(storage, self.rows)
+        if variant:  # pinned kernel (profiling commands: the same kernel as the timed run)
+            self.plan.set_variant(storage, variant)
 
     def step(self, timed=False):
         vf, torch = self.vf, self.torch
@@ -194,9 +196,9 @@ class DevicePipeline:
         return (e[0].elapsed_time(e[1]), e[1].elapsed_time(e[2]), e[2].elapsed_time(e[3]))
 
 
-def run_device(vf, frames, storage, steps, warmup, dist):
+def run_device(vf, frames, storage, steps, warmup, dist, variant=0):
     import torch
-    pipe = DevicePipeline(vf, frames, storage)
+    pipe = DevicePipeline(vf, frames, storage, variant)
     for _ in range(max(warmup, 1)):
         pipe.step()
     torch.cuda.synchronize()
@@ -513,6 +515,8 @@ def main():
     ap.add_argument("--cpu-sample", type=float, default=1.0)
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--skip-extras", action="store_true", help="only the primary line items")
+    ap.add_argument("--dd-variant", type=int, default=0,
+                    help="dedispersion kernel variant for the device legs (0: the autotuner's choice)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     dist = dist_init(args.gpus)
@@ -533,7 +537,7 @@ def main():
     t_gen = time.perf_counter() - t_gen
     data_s = args.duration
 
-    f32 = run_device(vf, frames, 0, args.steps, args.warmup, dist)
+    f32 = run_device(vf, frames, 0, args.steps, args.warmup, dist, args.dd_variant)
     rtf = world * data_s / (f32["ms"] / 1000.0)
     extras = {}
     f16 = None

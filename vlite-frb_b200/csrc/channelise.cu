@@ -305,7 +305,11 @@ int launch_channelise(const vfrb_chan_args& a, cudaStream_t s) {
   const size_t smem = kSmem;
   const bool aligned = (a.sample0 % 4) == 0;
   int dev = 0, nsm = 148;
-  if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  if (cudaGetDevice(&dev) != cudaSuccess ||
+      cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || nsm < 1) {
+    cudaGetLastError();
+    nsm = 148;
+  }
   const int grid = (int)std::min<long long>(a.nrows, (long long)nsm);
   cudaError_t e;
   if (aligned) {

@@ -723,8 +723,12 @@ int ddplan_autotune(vfrb_ddplan* pl, int storage, long long nt, float* times, cu
     cleanup();
     return VFRB_ERR_NOMEM;
   }
-  cudaMemsetAsync(fb, 0, (size_t)pl->nchan * rows * eb, s);
-  cudaMemsetAsync(w, 0, (size_t)pl->nchan * 4, s);
+  if (cudaMemsetAsync(fb, 0, (size_t)pl->nchan * rows * eb, s) != cudaSuccess ||
+      cudaMemsetAsync(w, 0, (size_t)pl->nchan * 4, s) != cudaSuccess) {
+    cudaGetLastError();
+    cleanup();
+    return VFRB_ERR_CUDA;
+  }
   vfrb_dd_args a{};
   a.fb = fb;
   a.storage = storage;
@@ -743,9 +747,13 @@ int ddplan_autotune(vfrb_ddplan* pl, int storage, long long nt, float* times, cu
   a.peak = st + 2 * pl->ndm;
   a.frb = stb;
   a.argmax = stb + pl->ndm;
-  cudaEvent_t e0, e1;
-  cudaEventCreate(&e0);
-  cudaEventCreate(&e1);
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) {
+    cudaGetLastError();
+    if (e0) cudaEventDestroy(e0);
+    cleanup();
+    return VFRB_ERR_CUDA;
+  }
   float best = 1e30f;
   int bestv = VFRB_DD_STAGED;
   if (times) times[VFRB_DD_AUTO] = -1.f;

@@ -1061,7 +1061,10 @@ int vfrb_plan_create(vfrb_plan** out, const vfrb_params* prm) {
   if (P.mode == VFRB_MODE_STREAM) {
     // whole rows per persistent channeliser CTA: a multiple of the SM count
     int nsm = 148;
-    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, P.device);
+    if (cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, P.device) != cudaSuccess || nsm < 1) {
+      cudaGetLastError();
+      nsm = 148;
+    }
     if (pl->launch_rows >= nsm) pl->launch_rows = pl->launch_rows / nsm * nsm;
     // a backlog of chunks is dedispersed in launches of about 4096 samples
     pl->batch_chunks = std::min<int64_t>(8, std::max<int64_t>(1, (4096 + pl->chunk_rows - 1) / pl->chunk_rows));
