@@ -415,6 +415,7 @@ struct RegGroup {
   int* d_gbase = nullptr;
   unsigned* d_gpack = nullptr;
   int* d_bmin = nullptr;
+  int bmin_mid_max = 0;             // max over CTA blocks of bmin at the middle channel
   unsigned char* d_gpat = nullptr;  // pattern id per (group, channel), D = 4 and 2
   long long n_generic = 0;          // (group, channel) pairs outside the pattern table
 };
@@ -583,11 +584,14 @@ static int pat_launch_t(const vfrb_ddplan* pl, const RegGroup& g, const vfrb_dd_
       cudaFuncSetAttribute(k_dedisp_pat<T, D, TT, SMAX>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return VFRB_ERR_CUDA;
   const long long ntime = (a.nt_out + NT - 1) / NT;
-  if (ntime > 65535) return VFRB_OK;  // time blocks run along grid y
-  dim3 grid((unsigned)g.nblocks, (unsigned)ntime);
+  // grid y runs time blocks shifted by each DM block's delay at the middle
+  // channel (see the kernel); the first and last rows hold empty CTAs
+  const long long ny = ntime + g.bmin_mid_max / NT;
+  if (ny > 65535) return VFRB_OK;
+  dim3 grid((unsigned)g.nblocks, (unsigned)ny);
   k_dedisp_pat<T, D, TT, SMAX><<<grid, kPatWarps * 32, smem, s>>>(k);
   const int st = cuda_status(cudaGetLastError());
-  if (st == VFRB_OK) *ntb = (int)grid.y;
+  if (st == VFRB_OK) *ntb = (int)ntime;
   return st;
 }
 
@@ -876,6 +880,7 @@ static int build_group(vfrb_ddplan* p, const int32_t* h_off, int D, int smax_all
   g.D = D;
   g.smax = smax;
   g.span = span;
+  for (int b = 0; b < nb; ++b) g.bmin_mid_max = std::max(g.bmin_mid_max, bm[(size_t)b * nchan + nchan / 2]);
   g.ngroups = ng;
   g.nblocks = nb;
   const bool with_pat = (D == 4 && smax <= VFRB_PAT4_SMAX) || (D == 2 && smax <= VFRB_PAT2_SMAX);

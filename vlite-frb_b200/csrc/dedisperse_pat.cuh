@@ -220,10 +220,15 @@ __global__ void __launch_bounds__(kPatWarps * 32, 2) k_dedisp_pat(const DdPatPar
   const int meta_q = 1 + (3 * kPatWarps * CH + kPatWarps + 3) / 4;
   int4* tiles = smp4 + meta_q;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  // DM blocks run along x (fastest), so the CTAs working on one time window
-  // are resident together and read its filterbank rows from L2, not DRAM
+  // DM blocks run along x (fastest); along y, DM block b takes time block
+  // y - shift_b, shift_b = its smallest delay at the middle channel in time
+  // blocks.  The CTAs resident together then read about the same rows of the
+  // middle channels (the rows a DM block needs move with its delay), which
+  // keeps the wave's working set near the L2 size; CTAs whose time block
+  // falls outside the output return at once.
   const int blk = blockIdx.x;
-  const int tb = blockIdx.y;
+  const int tb = (int)blockIdx.y - __ldg(p.bmin + (long long)blk * p.nchan + p.nchan / 2) / NT;
+  if (tb < 0 || (long long)tb * NT >= p.nt_out) return;
   const long long t0 = (long long)tb * NT;
   const int g = min(blk * kPatWarps + warp, p.ngroups - 1);
   const T* fb = reinterpret_cast<const T*>(p.fb);
