@@ -460,6 +460,15 @@ int vfrb_dada_set_eod(vfrb_dada* ring);
 int64_t vfrb_dada_read(vfrb_dada* ring, void* buf, uint64_t n, int timeout_ms);
 /* 1 when the writer has ended and every byte was read (ipcbuf_eod). */
 int vfrb_dada_eod(const vfrb_dada* ring);
+/* In-place reading: waits (bounded) for readable bytes and points *ptr at
+ * the longest contiguous run of them (at most max_n; it stops at the ring's
+ * end) without consuming them; returns its length, 0 at end of data, or
+ * -status.  vfrb_dada_release(n) consumes the first n acquired bytes. */
+int64_t vfrb_dada_acquire(vfrb_dada* ring, const uint8_t** ptr, uint64_t max_n, int timeout_ms);
+int vfrb_dada_release(vfrb_dada* ring, uint64_t n);
+/* Page-locks this process's mapping of the ring (needs a CUDA device), so
+ * vfrb_push_frames copies acquired bytes straight to the device. */
+int vfrb_dada_pin(vfrb_dada* ring);
 int vfrb_dada_close(vfrb_dada* ring);
 int vfrb_dada_destroy(uint32_t key);
 

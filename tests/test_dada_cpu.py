@@ -28,6 +28,9 @@ def _lib(vf):
     lib.vfrb_dada_eod.argtypes = [vp]
     lib.vfrb_dada_close.argtypes = [vp]
     lib.vfrb_dada_destroy.argtypes = [C.c_uint32]
+    lib.vfrb_dada_acquire.argtypes = [vp, C.POINTER(C.c_void_p), C.c_uint64, C.c_int]
+    lib.vfrb_dada_acquire.restype = C.c_int64
+    lib.vfrb_dada_release.argtypes = [vp, C.c_uint64]
     return lib
 
 
@@ -124,4 +127,52 @@ def test_writer_tool_feeds_reader(vf, tmp_path):
         if p.poll() is None:
             p.kill()
             p.wait()
+        lib.vfrb_dada_destroy(key)
+
+
+def test_ring_in_place_reading(vf):
+    """acquire/release: the bytes are read in place in contiguous runs that
+    stop at the ring's end, in order across wrap-around; releasing more than
+    was written is refused; 0 bytes at end of data; a bounded wait."""
+    lib = _lib(vf)
+    key = _key()
+    w = C.c_void_p()
+    assert lib.vfrb_dada_create(key, 1 << 14, C.byref(w)) == 0
+    try:
+        r = C.c_void_p()
+        assert lib.vfrb_dada_connect(key, C.byref(r)) == 0
+        p = C.c_void_p()
+        assert lib.vfrb_dada_acquire(r, C.byref(p), 1 << 20, 50) == -ERR_TIMEOUT  # nothing written yet
+        data = np.random.default_rng(5).integers(0, 256, 300_001, dtype=np.uint8)
+
+        def writer():
+            pos = 0
+            rng = np.random.default_rng(6)
+            while pos < data.size:
+                k = int(min(rng.integers(1, 9000), data.size - pos))
+                assert lib.vfrb_dada_write(w, data[pos:].ctypes.data, k, 5000) == k
+                pos += k
+            lib.vfrb_dada_set_eod(w)
+
+        t = threading.Thread(target=writer)
+        t.start()
+        got, runs = [], 0
+        rng = np.random.default_rng(7)
+        while True:
+            n = lib.vfrb_dada_acquire(r, C.byref(p), int(rng.integers(1, 20000)), 5000)
+            assert n >= 0
+            if n == 0:
+                break
+            assert n <= (1 << 14)
+            got.append(np.ctypeslib.as_array(C.cast(p, C.POINTER(C.c_uint8)), shape=(n,)).copy())
+            take = int(rng.integers(1, n + 1))  # consume part of the run; the rest is acquired again
+            got[-1] = got[-1][:take]
+            assert lib.vfrb_dada_release(r, take) == 0
+            runs += 1
+        t.join()
+        assert np.array_equal(np.concatenate(got), data) and runs > 20
+        assert lib.vfrb_dada_release(r, 1) != 0  # nothing left to release
+        lib.vfrb_dada_close(r)
+    finally:
+        lib.vfrb_dada_close(w)
         lib.vfrb_dada_destroy(key)

@@ -8,6 +8,10 @@
 // object named after the DADA key; the writer appends bytes and finally marks
 // end of data; the reader gets the bytes in order, and a short read means end
 // of data.  Every wait is bounded (timeout_ms) and reports VFRB_ERR_TIMEOUT.
+// A reader can also take the bytes in place (acquire / release) from a
+// mapping it page-locked (pin), so that vfrb_push_frames copies them to the
+// device straight from the ring, with no host copy in between.
+#include <cuda_runtime.h>
 #include <fcntl.h>
 #include <sys/mman.h>
 #include <sys/stat.h>
@@ -57,6 +61,7 @@ struct vfrb_dada {
   RingHdr* h = nullptr;
   uint8_t* data = nullptr;
   size_t map_bytes = 0;
+  bool pinned = false;
 };
 
 extern "C" {
@@ -180,6 +185,49 @@ int64_t vfrb_dada_read(vfrb_dada* d, void* buf, uint64_t n, int timeout_ms) {
   return (int64_t)done;
 }
 
+int64_t vfrb_dada_acquire(vfrb_dada* d, const uint8_t** ptr, uint64_t max_n, int timeout_ms) {
+  if (!d || !ptr || max_n == 0) return -VFRB_ERR_ARG;
+  const uint64_t cap = d->h->cap;
+  const double t0 = now_ms();
+  for (;;) {
+    const uint64_t r = d->h->rpos.load(std::memory_order_relaxed);
+    const uint64_t w = d->h->wpos.load(std::memory_order_acquire);
+    if (w != r) {
+      const uint64_t at = r & (cap - 1);
+      uint64_t k = w - r;
+      if (k > cap - at) k = cap - at;  // contiguous up to the ring's end
+      if (k > max_n) k = max_n;
+      *ptr = d->data + at;
+      return (int64_t)k;
+    }
+    if (d->h->eod.load(std::memory_order_acquire) && d->h->wpos.load(std::memory_order_acquire) == r) {
+      *ptr = nullptr;
+      return 0;
+    }
+    if (now_ms() - t0 > timeout_ms) return -VFRB_ERR_TIMEOUT;
+    nap();
+  }
+}
+
+int vfrb_dada_release(vfrb_dada* d, uint64_t n) {
+  if (!d) return VFRB_ERR_ARG;
+  const uint64_t r = d->h->rpos.load(std::memory_order_relaxed);
+  if (n > d->h->wpos.load(std::memory_order_acquire) - r) return VFRB_ERR_ARG;
+  d->h->rpos.store(r + n, std::memory_order_release);
+  return VFRB_OK;
+}
+
+int vfrb_dada_pin(vfrb_dada* d) {
+  if (!d) return VFRB_ERR_ARG;
+  if (d->pinned) return VFRB_OK;
+  if (cudaHostRegister(d->h, d->map_bytes, cudaHostRegisterDefault) != cudaSuccess) {
+    cudaGetLastError();
+    return VFRB_ERR_CUDA;
+  }
+  d->pinned = true;
+  return VFRB_OK;
+}
+
 int vfrb_dada_eod(const vfrb_dada* d) {
   if (!d) return VFRB_ERR_ARG;
   return d->h->eod.load(std::memory_order_acquire) &&
@@ -188,6 +236,7 @@ int vfrb_dada_eod(const vfrb_dada* d) {
 
 int vfrb_dada_close(vfrb_dada* d) {
   if (!d) return VFRB_ERR_ARG;
+  if (d->pinned && cudaHostUnregister(d->h) != cudaSuccess) cudaGetLastError();
   munmap(d->h, d->map_bytes);
   delete d;
   return VFRB_OK;

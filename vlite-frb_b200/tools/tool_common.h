@@ -54,6 +54,7 @@ struct Source {
   vfrb_dada* ring = nullptr;
   int timeout_ms = 300000;
   bool failed = false;
+  bool pinned = false;
   bool open(const char* path) {
     if (eq(path, "-")) {
       f = stdin;
@@ -70,8 +71,19 @@ struct Source {
       if ((now_s() - t0) * 1e3 > wait_ms) return false;
       usleep(20000);
     }
+    pinned = vfrb_dada_pin(ring) == VFRB_OK;  // else pushes go through the staging copy
     return true;
   }
+  // ring input: the next contiguous readable bytes in place (0 at end of data)
+  size_t acquire(const uint8_t** p, size_t max_n) {
+    const int64_t k = vfrb_dada_acquire(ring, p, max_n, timeout_ms);
+    if (k < 0) {
+      failed = true;
+      return 0;
+    }
+    return (size_t)k;
+  }
+  void release(size_t n) { vfrb_dada_release(ring, n); }
   size_t read(void* buf, size_t n) {
     if (ring) {
       const int64_t k = vfrb_dada_read(ring, buf, n, timeout_ms);
@@ -114,9 +126,13 @@ int run_stream(vfrb_plan* plan, Source& src, FILE* log, OnStart on_start, OnResu
     }
   };
   for (;;) {
-    const size_t n = src.read(buf.data(), buf.size());
+    // ring input is pushed in place (page-locked: copied straight to the
+    // device), file input through the read buffer
+    const uint8_t* p = buf.data();
+    const size_t n = src.ring ? src.acquire(&p, buf.size()) : src.read(buf.data(), buf.size());
     if (n == 0) break;
-    int st = vfrb_push_frames(plan, 0, buf.data(), n);
+    int st = vfrb_push_frames(plan, 0, p, n);
+    if (src.ring) src.release(n);
     if (st != VFRB_OK) {
       std::fprintf(log, "%s\n", vfrb_stream_log(plan, 0));
       std::fprintf(log, "processing stopped: %s\n", vfrb_strerror(st));
