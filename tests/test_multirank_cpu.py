@@ -84,3 +84,23 @@ def test_rank_leaving_is_detected_by_timeout():
     out = _run(2, 1)
     assert out[1][0] == "left"
     assert out[0][0] == "err", out  # the collective ends with an error, no hang
+
+
+def test_reference_arm_line_contract():
+    """`bench.py --impl reference` (the CPU port of the path, no GPU): one JSON
+    line with the arm's keys; e2e repeats the value with no copies."""
+    import json
+    import subprocess
+    import sys
+    r = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference", "--steps", "1",
+                        "--warmup", "1", "--cpu-sample", "0.05"], capture_output=True, text=True, timeout=600,
+                       cwd=ROOT)
+    assert r.returncode == 0, r.stderr[-2000:]
+    lines = [ln for ln in r.stdout.splitlines() if ln.startswith("{")]
+    assert len(lines) == 1
+    d = json.loads(lines[0])
+    assert d["impl"] == "reference" and d["unit"] == "s data/s" and d["higher_is_better"] is True
+    assert d["value"] > 0 and d["warmup"] >= 3 and d["steps"] == 1
+    cb = d["cpu_baseline"]
+    assert cb["kind"] in ("port", "reference") and cb["cores"] >= 1 and cb["value"] == d["value"] and cb["sample"]
+    assert d["e2e"] == {"value": d["value"], "unit": "s data/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}
