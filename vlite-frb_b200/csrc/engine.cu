@@ -28,10 +28,22 @@
 #include <string>
 #include <vector>
 
+#include <nvtx3/nvToolsExt.h>
+
 #include "vdif_reader.h"
 #include "vfrb_common.cuh"
 
 namespace vfrb {
+
+// NVTX range for profilers' timelines (header-only NVTX 3: a no-op unless a
+// tool is attached)
+struct Range {
+  explicit Range(const char* name) { nvtxRangePushA(name); }
+  ~Range() { nvtxRangePop(); }
+  Range(const Range&) = delete;
+  Range& operator=(const Range&) = delete;
+};
+
 size_t dedisperse_workspace_bytes_plan(const vfrb_ddplan* pl, long long nt_out);
 int launch_dedisperse_plan(const vfrb_ddplan* pl, const vfrb_dd_args& a, cudaStream_t s);
 int ddplan_create(vfrb_ddplan** out, const int32_t* h_off, int ndm, int nchan);
@@ -371,6 +383,7 @@ void consume_entries(StreamSt* s, int64_t first_needed) {
 // [r*S, (r+1)*S) of each pol, S = NAVE*TWONCHAN.
 int launch_rows(vfrb_plan* pl, StreamSt* s, int64_t row_first, int64_t nrows, float* out, int64_t out_row0,
                 unsigned mask) {
+  const Range nvtx_range("vfrb channelise");
   const vfrb_layout& L = pl->L;
   const int64_t S = (int64_t)L.nave * L.twonchan;
   const int64_t p0 = row_first * S, p1 = (row_first + nrows) * S;
@@ -473,6 +486,7 @@ int init_scale(vfrb_plan* pl, StreamSt* s, const float* raw, int64_t row0, unsig
 
 int run_bandpass(vfrb_plan* pl, StreamSt* s, const float* raw, int64_t in_row0, unsigned in_mask, int64_t nrows,
                  int64_t out_row0, float* tm_out, int subtract_mode = 0) {
+  const Range nvtx_range("vfrb bandpass");
   ST(init_scale(pl, s, raw, in_row0, in_mask));
   vfrb_bp_args a{};
   a.in = raw;
@@ -500,6 +514,7 @@ int run_bandpass(vfrb_plan* pl, StreamSt* s, const float* raw, int64_t in_row0, 
 // search) of the whole launch, fused (block mode); otherwise each output
 // chunk gets its statistics from chunk_stats (stream mode).
 int run_dedisp(vfrb_plan* pl, StreamSt* s, int64_t row0, int64_t nrows_valid, int64_t nt, bool kernel_stats) {
+  const Range nvtx_range("vfrb dedisperse");
   vfrb_dd_args a{};
   a.fb = s->d_cm;
   a.storage = pl->P.storage;
@@ -613,6 +628,7 @@ int emit(vfrb_plan* pl, StreamSt* s, int64_t seq, int64_t row0, int64_t nt, bool
 }
 
 int block_complete(vfrb_plan* pl, StreamSt* s) {
+  const Range nvtx_range("vfrb block");
   const vfrb_layout& L = pl->L;
   const int64_t nch = L.nchanout;
   if (pl->want_dd && pl->max_delay > 0)
@@ -682,6 +698,7 @@ int chunk_stats(vfrb_plan* pl, StreamSt* s, int64_t col0, int64_t nt) {
 
 // k output chunks of nt samples each with one dedispersion launch
 int stream_chunks(vfrb_plan* pl, StreamSt* s, int64_t k, int64_t nt) {
+  const Range nvtx_range("vfrb stream chunks");
   ST(run_dedisp(pl, s, s->rows_out, s->rows_bp - s->rows_out, k * nt, false));
   for (int64_t i = 0; i < k; ++i) {
     ST(chunk_stats(pl, s, i * nt, nt));
@@ -777,6 +794,7 @@ int64_t oldest_ref(const StreamSt* s) {
 
 // Copy `nf` whole frames to the ring, queue their headers, advance.
 int feed_frames(vfrb_plan* pl, StreamSt* s, const uint8_t* host, int64_t nf, bool pinned) {
+  const Range nvtx_range("vfrb feed frames");
   // page-locked input is copied in place, in quarters of the ring; other
   // input goes through the (smaller) staging buffers
   const int64_t batch_max =
