@@ -285,9 +285,11 @@ def run_serving(vf, storage, nstreams=16, paced_s=15.0, load=1.5, seed0=100):
     import torch
     from vlite_frb_b200 import synth
     fps, pair = 25600, 2 * 5032
+    # streams are admitted one by one as their data starts (vfrb_stream_open)
     plan = vf.Plan(dm_grid(), nave=NAVE, muoslowfreq=384.0, mode=vf.MODE_STREAM, storage=storage,
-                   chunk_seconds=1.0, ring_seconds=2.0, nstreams=nstreams,
+                   chunk_seconds=1.0, ring_seconds=2.0, nstreams=0,
                    outputs=vf.OUT_DMSTATS | vf.OUT_CANDS, cand_snr=7.0)
+    sid = []
     tchan = NAVE * 12500 / 128e6
     fill_s = (plan.max_delay + 1024) * tchan + 0.1
     buf = torch.empty(int(2.0 * fps + 2) * pair, dtype=torch.uint8, pin_memory=True)
@@ -313,7 +315,7 @@ def run_serving(vf, storage, nstreams=16, paced_s=15.0, load=1.5, seed0=100):
             total += f.numel()
             s["pair"] += npairs
             s["k"] += 1
-        plan.push(i, buf[:nbytes])
+        plan.push(sid[i], buf[:nbytes])
         s["tail"] = buf[nbytes:total].clone()
         s["sent"] += nbytes / (fps * pair)
         return nbytes / (fps * pair)
@@ -329,7 +331,11 @@ def run_serving(vf, storage, nstreams=16, paced_s=15.0, load=1.5, seed0=100):
                 lat.append(r["latency_ms"])
             cands.extend((r["stream"], c["dm_index"], c["t"], round(c["snr"], 4)) for c in r["cands"])
 
-    for i in range(nstreams):  # fill past the overlap, back to back
+    for i in range(nstreams):  # admit each stream and fill it past the overlap, back to back
+        k = plan.open_stream()
+        if k is None:
+            raise RuntimeError("stream %d not admitted" % i)
+        sid.append(k)
         while st[i]["sent"] < fill_s:
             push_chunk(i)
             drain(False)
@@ -345,8 +351,10 @@ def run_serving(vf, storage, nstreams=16, paced_s=15.0, load=1.5, seed0=100):
         drain(True)
     wall = time.perf_counter() - t0
     for i in range(nstreams):
-        plan.push(i, None)
+        plan.push(sid[i], None)
     drain(True, wait=True)
+    for i in range(nstreams):
+        plan.close_stream(sid[i])
     plan.close()
     return dict(lat=np.array(lat), cands=sorted(cands), offered=data_s / wall,
                 data_s=sum(s["sent"] for s in st))

@@ -326,7 +326,8 @@ typedef struct vfrb_params {
   float q_scale;                   /* int8 quantisation (z units -> counts)  */
   int32_t outputs;                 /* VFRB_OUT_* bits                        */
   int32_t fb_block;                /* block whose FB is returned (-1: all)   */
-  int32_t nstreams;                /* independent streams (antennas)         */
+  int32_t nstreams;                /* streams opened at creation (0..4096; more
+                                    * with vfrb_stream_open)               */
   float chunk_seconds;             /* streaming output chunk                 */
   float ring_seconds;              /* device raw-frame ring per stream       */
   float cand_snr;                  /* candidate threshold (peak SNR)         */
@@ -416,6 +417,18 @@ int64_t vfrb_plan_device_bytes(const vfrb_plan* plan);
  * input is copied to the device directly, other input through a staging
  * buffer; `bytes` may be reused as soon as the call returns. */
 int vfrb_push_frames(vfrb_plan* plan, int stream, const uint8_t* bytes, size_t nbytes);
+
+/* Streams opened and closed while others run (serving).  vfrb_stream_open
+ * admits one more stream if its device bytes fit the budget (device_bytes,
+ * or 90% of the free memory) beside the open streams, and returns its id
+ * (ids are never reused); VFRB_ERR_NOMEM when it does not fit -- retry after
+ * another stream has closed.  vfrb_stream_close ends the stream's data (as
+ * vfrb_push_frames with nbytes 0) and, once all its results have been
+ * polled, frees its memory and returns VFRB_OK; before that it returns
+ * VFRB_PENDING.  A result of the stream returned by the last vfrb_poll is
+ * invalid after the close. */
+int vfrb_stream_open(vfrb_plan* plan, int* stream);
+int vfrb_stream_close(vfrb_plan* plan, int stream);
 
 /* Next completed result in submission order.  Returns VFRB_OK with *out
  * filled (host buffers owned by the plan, valid until the next poll),

@@ -273,6 +273,75 @@ def test_stream_split_invariance_and_isolation(vf):
         assert all(r["device_errors"] == 0 for r in mixed[s])
 
 
+def test_streams_open_close_and_admission(vf):
+    """Serving: streams are opened while others run and closed when done;
+    admission refuses a stream whose device memory does not fit the budget
+    until another has closed and freed its memory; every stream's series
+    equal its series run alone, bit for bit."""
+    dms = np.arange(0, 6.0, 0.5, dtype=np.float32)
+    bufs = [_vdif(0.9, seed=200 + i) for i in range(3)]
+    alone = [np.concatenate([r["dd"] for r in _stream_run(vf, dms, [b])[1][0]], axis=1) for b in bufs]
+    kw = dict(nave=2, muoslowfreq=384.0, mode=vf.MODE_STREAM, chunk_seconds=0.25, outputs=vf.OUT_DEDISP)
+    probe = vf.Plan(dms, nstreams=1, **kw)
+    one = probe.device_bytes
+    probe.close()
+    plan = vf.Plan(dms, nstreams=0, device_bytes=int(2.5 * one), **kw)
+    assert plan.device_bytes == 0
+    a, b = plan.open_stream(), plan.open_stream()
+    assert (a, b) == (0, 1) and plan.device_bytes == 2 * one
+    assert plan.open_stream() is None  # a third does not fit beside two
+    got = {}
+
+    def take(r):
+        if r is not None:
+            got.setdefault(r["stream"], []).append(r["dd"])
+
+    half = len(bufs[0]) // 2 + 777  # cut inside a frame
+    plan.push(a, bufs[0][:half])
+    plan.push(b, bufs[1][:half])
+    plan.push(a, bufs[0][half:])
+    while not plan.close_stream(a):  # ends stream a; frees it once its results are polled
+        take(plan.poll(wait=True))
+    assert plan.device_bytes == one
+    with pytest.raises(vf.VfrbError):
+        plan.push(a, bufs[0][:10064])
+    c = plan.open_stream()
+    assert c == 2
+    plan.push(c, bufs[2])
+    plan.push(b, bufs[1][half:])
+    plan.push(b, None)
+    plan.push(c, None)
+    for r in plan.drain():
+        take(r)
+    for i, sid in enumerate((a, b, c)):
+        assert np.array_equal(np.concatenate(got[sid], axis=1), alone[i]), sid
+    assert plan.close_stream(b) and plan.close_stream(c) and plan.device_bytes == 0
+    plan.close()
+
+
+def test_garbage_input_fails_cleanly(vf):
+    """Bytes that are not VDIF end the stream at the reader (the reference's
+    initframe01 failure, status 2) with no result and nothing launched on
+    bad data; the plan stays usable for the next stream."""
+    dms = np.arange(0, 6.0, 0.5, dtype=np.float32)
+    plan = vf.Plan(dms, nave=2, muoslowfreq=384.0, mode=vf.MODE_STREAM, chunk_seconds=0.25, nstreams=1,
+                   outputs=vf.OUT_DEDISP)
+    garbage = np.random.default_rng(9).integers(0, 256, 3_000_000, dtype=np.uint8)
+    for data in (garbage, None):
+        try:
+            plan.push(0, data)
+        except vf.VfrbError as e:
+            assert e.status == 2
+            break
+    assert plan.drain() == []
+    sid = plan.open_stream()
+    plan.push(sid, _vdif(0.9, seed=5))
+    plan.push(sid, None)
+    res = plan.drain()
+    assert res and all(r["stream"] == sid and r["device_errors"] == 0 for r in res)
+    plan.close()
+
+
 def test_stream_fp16_form(vf):
     """FP16 storage: series within 3e-3 rms of FP32, identical candidates."""
     dms = np.arange(0, 12.0, 0.25, dtype=np.float32)

@@ -71,6 +71,44 @@ def _assert_fb_close(got, ref, elementwise=False, tol=1e-5):
         assert rel.max() <= 1e-5
 
 
+def test_channelise_tones_and_impulses(vf, O):
+    """Known inputs through the 12500-point transform (nave 1, full band):
+    an on-bin tone in pol 0 only, an off-bin tone in pol 1 only (leakage),
+    one impulse per pol (flat spectrum) and both tones over noise.  Against
+    the FP64 oracle, plus the spectra's own structure: the tone's channel,
+    the flat impulse spectrum."""
+    torch = _torch()
+    n = 12500
+    t = np.arange(n)
+    quiet = np.full(n, 128.0)
+    tone0 = 128 + 60 * np.cos(2 * np.pi * 1000 * t / n)
+    tone1 = 128 + 50 * np.sin(2 * np.pi * 3001.5 * t / n + 0.3)
+    imp0, imp1 = quiet.copy(), quiet.copy()
+    imp0[17] = 255
+    imp1[6000] = 0
+    rng = np.random.default_rng(4)
+    noise = rng.normal(0, 12, (2, n))
+    rows = [(tone0, quiet), (quiet, tone1), (imp0, imp1), (tone0 + noise[0], tone1 + noise[1])]
+    p0 = np.concatenate([np.clip(np.round(a), 0, 255) for a, _ in rows]).astype(np.uint8)
+    p1 = np.concatenate([np.clip(np.round(b), 0, 255) for _, b in rows]).astype(np.uint8)
+    L = vf.layout(nave=1, muoslowfreq=384.0)
+    Lo = O.Layout(nave=1, muoslowfreq=384.0)
+    ref = O.channelise(p0, p1, Lo)
+    dev = torch.device("cuda")
+    d = torch.from_numpy(np.concatenate([p0, p1])).to(dev)  # pol 0 payloads, then pol 1 payloads
+    ns = len(p0) // 5000
+    s0 = torch.arange(ns, dtype=torch.int64, device=dev) * 5000
+    got = vf.channelise(d, s0, s0 + len(p0), 0, 4, L).cpu().numpy().astype(np.float64)
+    _assert_fb_close(got, ref)
+    assert int(np.argmax(got[0])) == 1000 - L.nskip  # the on-bin tone's channel
+    assert got[0, 1000 - L.nskip] > 1e4 * np.median(got[0])
+    pk = int(np.argmax(got[1])) + L.nskip  # off-bin: the power sits in bins 3001 and 3002
+    assert pk in (3001, 3002) and got[1, 3001 - L.nskip] / got[1, 3002 - L.nskip] == pytest.approx(1.0, rel=0.05)
+    flat = got[2]
+    assert flat.max() / flat.min() == pytest.approx(1.0, abs=1e-5)  # |127|^2 + |128|^2 in every bin
+    assert flat[0] == pytest.approx((127.0 ** 2 + 128.0 ** 2) / L.nfreq, rel=1e-6)
+
+
 def test_channelise_unaligned_and_ring(vf, O):
     """sample0 not a multiple of 4 (byte path) and output into a wrapped ring."""
     torch = _torch()

@@ -350,6 +350,7 @@ OUT_DEDISP, OUT_DMSTATS, OUT_SIGMA, OUT_CHANSTATS, OUT_FB, OUT_CANDS, OUT_FLAGS 
 ROW_INVALID, ROW_FILL = 1, 2
 BP_CAL, BP_FULL = 0, 1
 VFRB_PENDING = 9
+ERR_NOMEM = 6
 
 
 class Params(C.Structure):
@@ -409,6 +410,8 @@ _lib.vfrb_plan_device_bytes.restype = C.c_int64
 _lib.vfrb_plan_device_bytes.argtypes = [C.c_void_p]
 _lib.vfrb_push_frames.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_size_t]
 _lib.vfrb_poll.argtypes = [C.c_void_p, C.POINTER(Result), C.c_int]
+_lib.vfrb_stream_open.argtypes = [C.c_void_p, C.POINTER(C.c_int)]
+_lib.vfrb_stream_close.argtypes = [C.c_void_p, C.c_int]
 _lib.vfrb_stream_log.restype = C.c_char_p
 _lib.vfrb_stream_log.argtypes = [C.c_void_p, C.c_int]
 
@@ -446,6 +449,25 @@ class Plan:
     @property
     def device_bytes(self):
         return int(_lib.vfrb_plan_device_bytes(self._h))
+
+    def open_stream(self):
+        """Admit one more stream (vfrb_stream_open); returns its id, or None
+        when its device memory does not fit the budget now."""
+        i = C.c_int(-1)
+        st = _lib.vfrb_stream_open(self._h, C.byref(i))
+        if st == ERR_NOMEM:
+            return None
+        _check(st, "vfrb_stream_open")
+        return i.value
+
+    def close_stream(self, stream: int) -> bool:
+        """End a stream and free it once its results are polled
+        (vfrb_stream_close): True when freed, False while results remain."""
+        st = _lib.vfrb_stream_close(self._h, stream)
+        if st == VFRB_PENDING:
+            return False
+        _check(st, "vfrb_stream_close")
+        return True
 
     def push(self, stream: int, data):
         """data: bytes / numpy uint8 / torch uint8 CPU tensor (pinned or not); None = end of data."""

@@ -73,7 +73,8 @@ static double now_ms() {
     if (st_) return st_; \
   } while (0)
 
-constexpr int kStash = 1024;   // gap-revealing frames kept aside per stream
+constexpr int kStash = 1024;       // gap-revealing frames kept aside per stream
+constexpr int kMaxStreams = 4096;  // stream ids over a plan's life
 constexpr int kSlotBufs = 32;  // rotating slot-table uploads in flight (host runs ahead of the GPU)
 constexpr int kStageBufs = 2;  // rotating staging buffers for pageable input
 
@@ -114,6 +115,27 @@ __global__ void k_uniform_scale(const float* var, int nchan, float* w, float* in
   for (int c = threadIdx.x; c < nchan; c += blockDim.x) inv[c] = 1.f / S;
 }
 
+// Device and page-locked host memory, events and CUDA streams one stream
+// owns; released together when the stream is closed or the plan destroyed.
+struct Owned {
+  std::vector<void*> dev, host;
+  std::vector<cudaEvent_t> ev;
+  std::vector<cudaStream_t> cs;
+  int64_t dev_bytes = 0;
+  void release() {
+    for (auto s : cs) cudaStreamSynchronize(s);
+    for (auto s : cs) cudaStreamDestroy(s);
+    for (auto e : ev) cudaEventDestroy(e);
+    for (auto p : dev) cudaFree(p);
+    for (auto p : host) cudaFreeHost(p);
+    cs.clear();
+    ev.clear();
+    dev.clear();
+    host.clear();
+    dev_bytes = 0;
+  }
+};
+
 struct ResultSlot {
   vfrb_result r{};
   float *dd = nullptr, *dds = nullptr, *ave = nullptr, *sig = nullptr, *peak = nullptr, *fb = nullptr;
@@ -140,6 +162,7 @@ struct SlotBuf {
 
 struct StreamSt {
   int id = 0;
+  Owned res;
   cudaStream_t cs = nullptr;   // compute
   cudaStream_t xs = nullptr;   // host-to-device copies
   cudaEvent_t ev_copied = nullptr, ev_consumed = nullptr;
@@ -225,14 +248,11 @@ struct vfrb_plan {
   int64_t launch_rows = 0;  // most rows one channelise launch produces
   int64_t batch_chunks = 1; // stream mode: most output chunks one dedispersion launch covers
   int ncolstatblk = 0, nstatblks = 0;
-  int64_t dev_bytes = 0;
-  std::vector<std::unique_ptr<StreamSt>> st;
+  int64_t ring_frames = 0, R1 = 0, R2 = 0;  // per-stream geometry (admission, open)
+  std::vector<std::unique_ptr<StreamSt>> st;  // by stream id; null once closed
   std::deque<ResultSlot*> queue;  // submission order
   ResultSlot* held = nullptr;     // returned by the last poll
   std::string logtmp;
-  std::vector<void*> dev_allocs, host_allocs;
-  std::vector<cudaEvent_t> events;
-  std::vector<cudaStream_t> streams;
 };
 
 namespace {
@@ -247,33 +267,39 @@ bool is_pinned(const void* p) {
 }
 
 template <typename T>
-int dmalloc(vfrb_plan* pl, T** p, size_t bytes) {
+int dmalloc(Owned& o, T** p, size_t bytes) {
   if (bytes == 0) bytes = 16;
   if (cudaMalloc((void**)p, bytes) != cudaSuccess) {
     cudaGetLastError();
     *p = nullptr;
     return VFRB_ERR_NOMEM;
   }
-  pl->dev_allocs.push_back((void*)*p);
-  pl->dev_bytes += (int64_t)bytes;
+  o.dev.push_back((void*)*p);
+  o.dev_bytes += (int64_t)bytes;
   return VFRB_OK;
 }
 
 template <typename T>
-int hmalloc(vfrb_plan* pl, T** p, size_t bytes) {
+int hmalloc(Owned& o, T** p, size_t bytes) {
   if (bytes == 0) bytes = 16;
   if (cudaHostAlloc((void**)p, bytes, cudaHostAllocDefault) != cudaSuccess) {
     cudaGetLastError();
     *p = nullptr;
     return VFRB_ERR_NOMEM;
   }
-  pl->host_allocs.push_back((void*)*p);
+  o.host.push_back((void*)*p);
   return VFRB_OK;
 }
 
-int mkevent(vfrb_plan* pl, cudaEvent_t* e) {
+int mkevent(Owned& o, cudaEvent_t* e) {
   CK(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
-  pl->events.push_back(*e);
+  o.ev.push_back(*e);
+  return VFRB_OK;
+}
+
+int mkstream(Owned& o, cudaStream_t* s) {
+  CK(cudaStreamCreateWithFlags(s, cudaStreamNonBlocking));
+  o.cs.push_back(*s);
   return VFRB_OK;
 }
 
@@ -319,28 +345,28 @@ int alloc_slot(vfrb_plan* pl, StreamSt* s, ResultSlot** out) {
   const int64_t nch = pl->L.nchanout;
   const int64_t nt = P.mode == VFRB_MODE_BLOCK ? pl->nt_block : pl->chunk_rows;
   if (pl->want_dd) {
-    if (want(pl, VFRB_OUT_DEDISP)) ST(hmalloc(pl, &r->dd, (size_t)pl->ndm * nt * 4));
-    if (want(pl, VFRB_OUT_SIGMA)) ST(hmalloc(pl, &r->dds, (size_t)pl->ndm * nt * 4));
-    ST(hmalloc(pl, &r->ave, (size_t)pl->ndm * 4));
-    ST(hmalloc(pl, &r->sig, (size_t)pl->ndm * 4));
-    ST(hmalloc(pl, &r->peak, (size_t)pl->ndm * 4));
-    ST(hmalloc(pl, &r->frb, (size_t)pl->ndm * 4));
-    ST(hmalloc(pl, &r->arg, (size_t)pl->ndm * 4));
+    if (want(pl, VFRB_OUT_DEDISP)) ST(hmalloc(s->res, &r->dd, (size_t)pl->ndm * nt * 4));
+    if (want(pl, VFRB_OUT_SIGMA)) ST(hmalloc(s->res, &r->dds, (size_t)pl->ndm * nt * 4));
+    ST(hmalloc(s->res, &r->ave, (size_t)pl->ndm * 4));
+    ST(hmalloc(s->res, &r->sig, (size_t)pl->ndm * 4));
+    ST(hmalloc(s->res, &r->peak, (size_t)pl->ndm * 4));
+    ST(hmalloc(s->res, &r->frb, (size_t)pl->ndm * 4));
+    ST(hmalloc(s->res, &r->arg, (size_t)pl->ndm * 4));
     if (boxcar_on(pl)) {
-      ST(hmalloc(pl, &r->bsnr, (size_t)pl->ndm * 4));
-      ST(hmalloc(pl, &r->bt, (size_t)pl->ndm * 4));
-      ST(hmalloc(pl, &r->bw, (size_t)pl->ndm * 4));
+      ST(hmalloc(s->res, &r->bsnr, (size_t)pl->ndm * 4));
+      ST(hmalloc(s->res, &r->bt, (size_t)pl->ndm * 4));
+      ST(hmalloc(s->res, &r->bw, (size_t)pl->ndm * 4));
     }
   }
-  if (P.mode == VFRB_MODE_BLOCK && want(pl, VFRB_OUT_FB)) ST(hmalloc(pl, &r->fb, (size_t)pl->L.maxnt * nch * 4));
+  if (P.mode == VFRB_MODE_BLOCK && want(pl, VFRB_OUT_FB)) ST(hmalloc(s->res, &r->fb, (size_t)pl->L.maxnt * nch * 4));
   if (P.mode == VFRB_MODE_BLOCK && want(pl, VFRB_OUT_CHANSTATS)) {
-    ST(hmalloc(pl, &r->cave, (size_t)pl->nstatblks * nch * 4));
-    ST(hmalloc(pl, &r->csig, (size_t)pl->nstatblks * nch * 4));
-    ST(hmalloc(pl, &r->cout, (size_t)pl->nstatblks * nch * 4));
-    ST(hmalloc(pl, &r->csk, (size_t)pl->nstatblks * nch * 4));
+    ST(hmalloc(s->res, &r->cave, (size_t)pl->nstatblks * nch * 4));
+    ST(hmalloc(s->res, &r->csig, (size_t)pl->nstatblks * nch * 4));
+    ST(hmalloc(s->res, &r->cout, (size_t)pl->nstatblks * nch * 4));
+    ST(hmalloc(s->res, &r->csk, (size_t)pl->nstatblks * nch * 4));
   }
-  ST(hmalloc(pl, &r->err, 4));
-  ST(mkevent(pl, &r->ev));
+  ST(hmalloc(s->res, &r->err, 4));
+  ST(mkevent(s->res, &r->ev));
   *out = r.get();
   s->slots.push_back(std::move(r));
   return VFRB_OK;
@@ -870,80 +896,78 @@ int feed_frames(vfrb_plan* pl, StreamSt* s, const uint8_t* host, int64_t nf, boo
 
 int free_plan(vfrb_plan* pl) {
   if (!pl) return VFRB_OK;
-  for (auto s : pl->streams) cudaStreamSynchronize(s);
-  for (auto s : pl->streams) cudaStreamDestroy(s);
-  for (auto e : pl->events) cudaEventDestroy(e);
-  for (auto p : pl->dev_allocs) cudaFree(p);
-  for (auto p : pl->host_allocs) cudaFreeHost(p);
+  for (auto& s : pl->st)
+    if (s) s->res.release();
   if (pl->dd) ddplan_destroy(pl->dd);
   delete pl;
   return VFRB_OK;
 }
 
+// Appends stream `id` to pl->st first, so a failure part-way leaves its
+// allocations where free_plan (or vfrb_stream_open) releases them.
 int create_stream(vfrb_plan* pl, int id, int64_t ring_frames, int64_t R1, int64_t R2) {
-  auto s = std::make_unique<StreamSt>();
+  pl->st.push_back(std::make_unique<StreamSt>());
+  StreamSt* s = pl->st.back().get();
   const vfrb_params& P = pl->P;
   const vfrb_layout& L = pl->L;
   const int64_t nch = L.nchanout;
   s->id = id;
   s->reader = std::make_unique<PairReader>(P.reader == VFRB_READER_TS ? PairReader::TS : PairReader::PIPE,
                                            P.dada_skip != 0);
-  CK(cudaStreamCreateWithFlags(&s->cs, cudaStreamNonBlocking));
-  pl->streams.push_back(s->cs);
-  CK(cudaStreamCreateWithFlags(&s->xs, cudaStreamNonBlocking));
-  pl->streams.push_back(s->xs);
-  ST(mkevent(pl, &s->ev_copied));
-  ST(mkevent(pl, &s->ev_consumed));
-  for (auto& e : s->rel_ev) ST(mkevent(pl, &e));
+  ST(mkstream(s->res, &s->cs));
+  ST(mkstream(s->res, &s->xs));
+  ST(mkevent(s->res, &s->ev_copied));
+  ST(mkevent(s->res, &s->ev_consumed));
+  for (auto& e : s->rel_ev) ST(mkevent(s->res, &e));
   CK(cudaEventRecord(s->ev_consumed, s->cs));
   s->ring_frames = ring_frames;
   s->finv.assign((size_t)ring_frames, 0);
-  ST(dmalloc(pl, &s->d_frames, (size_t)ring_frames * kFrameLen + (size_t)kStash * kDataLen));
+  ST(dmalloc(s->res, &s->d_frames, (size_t)ring_frames * kFrameLen + (size_t)kStash * kDataLen));
   s->stage_frames = (size_t)std::min<int64_t>(ring_frames / 4, 8192);
   for (int k = 0; k < kStageBufs; ++k) {
-    ST(hmalloc(pl, &s->h_stage[k], s->stage_frames * kFrameLen));
-    ST(mkevent(pl, &s->stage_ev[k]));
+    ST(hmalloc(s->res, &s->h_stage[k], s->stage_frames * kFrameLen));
+    ST(mkevent(s->res, &s->stage_ev[k]));
     CK(cudaEventRecord(s->stage_ev[k], s->xs));
   }
   s->slots_cap = (pl->launch_rows * L.nave * (int64_t)L.twonchan) / kDataLen + 4;
   for (auto& b : s->sb) {
-    ST(hmalloc(pl, &b.h, sizeof(int64_t) * 2 * s->slots_cap));
-    ST(dmalloc(pl, &b.d, sizeof(int64_t) * 2 * s->slots_cap));
-    ST(mkevent(pl, &b.ev));
-    ST(mkevent(pl, &b.ev_used));
+    ST(hmalloc(s->res, &b.h, sizeof(int64_t) * 2 * s->slots_cap));
+    ST(dmalloc(s->res, &b.d, sizeof(int64_t) * 2 * s->slots_cap));
+    ST(mkevent(s->res, &b.ev));
+    ST(mkevent(s->res, &b.ev_used));
     CK(cudaEventRecord(b.ev, s->cs));
     CK(cudaEventRecord(b.ev_used, s->cs));
   }
-  ST(dmalloc(pl, &s->d_err, 4));
+  ST(dmalloc(s->res, &s->d_err, 4));
   CK(cudaMemsetAsync(s->d_err, 0, 4, s->cs));
-  ST(dmalloc(pl, &s->d_w, nch * 4));
-  ST(dmalloc(pl, &s->d_inv, nch * 4));
-  ST(dmalloc(pl, &s->d_var, nch * 4));
-  ST(dmalloc(pl, &s->d_scr, nch * 128 * 4));
+  ST(dmalloc(s->res, &s->d_w, nch * 4));
+  ST(dmalloc(s->res, &s->d_inv, nch * 4));
+  ST(dmalloc(s->res, &s->d_var, nch * 4));
+  ST(dmalloc(s->res, &s->d_scr, nch * 128 * 4));
   const size_t sb = storage_bytes(P.storage);
   int64_t nt = 0;
   if (P.mode == VFRB_MODE_BLOCK) {
-    ST(dmalloc(pl, &s->d_fb_tm, (size_t)L.maxnt * nch * 4));
+    ST(dmalloc(s->res, &s->d_fb_tm, (size_t)L.maxnt * nch * 4));
     CK(cudaMemsetAsync(s->d_fb_tm, 0, (size_t)L.maxnt * nch * 4, s->cs));
-    if (pl->want_dd && pl->max_delay > 0) ST(dmalloc(pl, &s->d_left, (size_t)pl->max_delay * nch * 4));
+    if (pl->want_dd && pl->max_delay > 0) ST(dmalloc(s->res, &s->d_left, (size_t)pl->max_delay * nch * 4));
     s->cm_stride = ((int64_t)L.maxnt + 15) / 16 * 16;
     s->cm_mask = 0xffffffffu;
-    ST(dmalloc(pl, &s->d_cm, (size_t)nch * s->cm_stride * sb));
-    if (want(pl, VFRB_OUT_FB)) ST(dmalloc(pl, &s->d_fbt, (size_t)L.maxnt * nch * 4));
+    ST(dmalloc(s->res, &s->d_cm, (size_t)nch * s->cm_stride * sb));
+    if (want(pl, VFRB_OUT_FB)) ST(dmalloc(s->res, &s->d_fbt, (size_t)L.maxnt * nch * 4));
     if (want(pl, VFRB_OUT_CHANSTATS)) {
-      ST(dmalloc(pl, &s->d_cave, (size_t)pl->nstatblks * nch * 4));
-      ST(dmalloc(pl, &s->d_csig, (size_t)pl->nstatblks * nch * 4));
-      ST(dmalloc(pl, &s->d_cout, (size_t)pl->nstatblks * nch * 4));
-      ST(dmalloc(pl, &s->d_csk, (size_t)pl->nstatblks * nch * 4));
+      ST(dmalloc(s->res, &s->d_cave, (size_t)pl->nstatblks * nch * 4));
+      ST(dmalloc(s->res, &s->d_csig, (size_t)pl->nstatblks * nch * 4));
+      ST(dmalloc(s->res, &s->d_cout, (size_t)pl->nstatblks * nch * 4));
+      ST(dmalloc(s->res, &s->d_csk, (size_t)pl->nstatblks * nch * 4));
     }
     nt = pl->nt_block;
     s->rflags.assign((size_t)L.maxnt, 0);
   } else {
     s->R1 = R1;
-    ST(dmalloc(pl, &s->d_raw, (size_t)R1 * nch * 4));
+    ST(dmalloc(s->res, &s->d_raw, (size_t)R1 * nch * 4));
     s->cm_stride = R2;
     s->cm_mask = (unsigned)(R2 - 1);
-    ST(dmalloc(pl, &s->d_cm, (size_t)nch * R2 * sb));
+    ST(dmalloc(s->res, &s->d_cm, (size_t)nch * R2 * sb));
     CK(cudaMemsetAsync(s->d_cm, 0, (size_t)nch * R2 * sb, s->cs));
     nt = pl->chunk_rows * pl->batch_chunks;
     // rows from the oldest not yet emitted to the newest channelised: at
@@ -953,22 +977,22 @@ int create_stream(vfrb_plan* pl, int id, int64_t ring_frames, int64_t R1, int64_
   }
   if (pl->want_dd) {
     s->out_stride = nt;
-    ST(dmalloc(pl, &s->d_out, (size_t)pl->ndm * nt * 4));
-    if (want(pl, VFRB_OUT_SIGMA)) ST(dmalloc(pl, &s->d_sig, (size_t)pl->ndm * nt * 4));
-    ST(dmalloc(pl, &s->d_ave, pl->ndm * 4));
-    ST(dmalloc(pl, &s->d_sgm, pl->ndm * 4));
-    ST(dmalloc(pl, &s->d_peak, pl->ndm * 4));
-    ST(dmalloc(pl, &s->d_frb, pl->ndm * 4));
-    ST(dmalloc(pl, &s->d_arg, pl->ndm * 4));
+    ST(dmalloc(s->res, &s->d_out, (size_t)pl->ndm * nt * 4));
+    if (want(pl, VFRB_OUT_SIGMA)) ST(dmalloc(s->res, &s->d_sig, (size_t)pl->ndm * nt * 4));
+    ST(dmalloc(s->res, &s->d_ave, pl->ndm * 4));
+    ST(dmalloc(s->res, &s->d_sgm, pl->ndm * 4));
+    ST(dmalloc(s->res, &s->d_peak, pl->ndm * 4));
+    ST(dmalloc(s->res, &s->d_frb, pl->ndm * 4));
+    ST(dmalloc(s->res, &s->d_arg, pl->ndm * 4));
     if (boxcar_on(pl)) {
-      ST(dmalloc(pl, &s->d_bsnr, pl->ndm * 4));
-      ST(dmalloc(pl, &s->d_bt, pl->ndm * 4));
-      ST(dmalloc(pl, &s->d_bw, pl->ndm * 4));
+      ST(dmalloc(s->res, &s->d_bsnr, pl->ndm * 4));
+      ST(dmalloc(s->res, &s->d_bt, pl->ndm * 4));
+      ST(dmalloc(s->res, &s->d_bw, pl->ndm * 4));
     }
     s->ws_bytes = dedisperse_workspace_bytes_plan(pl->dd, nt);
-    ST(dmalloc(pl, &s->d_ws, s->ws_bytes));
+    ST(dmalloc(s->res, &s->d_ws, s->ws_bytes));
   }
-  StreamSt* sp = s.get();
+  StreamSt* sp = s;
   // a gap-revealing frame is copied aside: it is used again NSKIP pairs later
   s->reader->on_gap = [pl, sp](int64_t v) -> int64_t {
     if (v < 0) return v;
@@ -984,7 +1008,6 @@ int create_stream(vfrb_plan* pl, int id, int64_t ring_frames, int64_t R1, int64_
     (void)pl;
     return -2 - k;
   };
-  pl->st.push_back(std::move(s));
   return VFRB_OK;
 }
 
@@ -1024,7 +1047,7 @@ int vfrb_plan_create(vfrb_plan** out, const vfrb_params* prm) {
     free_plan(pl);
     return st;
   };
-  if (P.nstreams < 1 || P.nstreams > 4096 || (P.mode != VFRB_MODE_BLOCK && P.mode != VFRB_MODE_STREAM) ||
+  if (P.nstreams < 0 || P.nstreams > kMaxStreams || (P.mode != VFRB_MODE_BLOCK && P.mode != VFRB_MODE_STREAM) ||
       P.storage < VFRB_F32 || P.storage > VFRB_I8 || P.ring_seconds <= 0.f || P.q_scale <= 0.f ||
       P.boxcar_max < 0 || P.boxcar_max > 65536 || (P.bp_mode != VFRB_BP_CAL && P.bp_mode != VFRB_BP_FULL) ||
       (P.zero_dm != 0 && P.zero_dm != 1))
@@ -1090,6 +1113,9 @@ int vfrb_plan_create(vfrb_plan** out, const vfrb_params* prm) {
   const int64_t R1 = (int64_t)pow2_at_least((unsigned long long)(pl->launch_rows + 512));
   const int64_t R2 = (int64_t)pow2_at_least(
       (unsigned long long)(pl->max_delay + pl->chunk_rows * pl->batch_chunks + pl->launch_rows + 512));
+  pl->ring_frames = ring_frames;
+  pl->R1 = R1;
+  pl->R2 = R2;
   // admission by device memory
   const int64_t need = stream_bytes(pl, ring_frames, R1, R2) * P.nstreams;
   size_t fr = 0, tot = 0;
@@ -1106,7 +1132,10 @@ int vfrb_plan_create(vfrb_plan** out, const vfrb_params* prm) {
   if (pl->want_dd && !(P.outputs & VFRB_OUT_SIGMA)) {
     // pick the fastest dedispersion kernel variant for this grid and chunk
     const int64_t nt = P.mode == VFRB_MODE_BLOCK ? pl->nt_block : pl->chunk_rows;
-    st = ddplan_autotune(pl->dd, P.storage, nt, nullptr, pl->st[0]->cs);
+    cudaStream_t ts = nullptr;
+    if (cudaStreamCreateWithFlags(&ts, cudaStreamNonBlocking) != cudaSuccess) return fail(VFRB_ERR_CUDA);
+    st = ddplan_autotune(pl->dd, P.storage, nt, nullptr, ts);
+    cudaStreamDestroy(ts);
     if (st) return fail(st);
   }
   *out = pl;
@@ -1122,10 +1151,58 @@ int vfrb_plan_layout(const vfrb_plan* pl, vfrb_layout* L, int32_t* max_delay) {
   return VFRB_OK;
 }
 
-int64_t vfrb_plan_device_bytes(const vfrb_plan* pl) { return pl ? pl->dev_bytes : -1; }
+int64_t vfrb_plan_device_bytes(const vfrb_plan* pl) {
+  if (!pl) return -1;
+  int64_t b = 0;
+  for (auto& s : pl->st)
+    if (s) b += s->res.dev_bytes;
+  return b;
+}
+
+int vfrb_stream_open(vfrb_plan* pl, int* stream) {
+  if (!pl || !stream) return VFRB_ERR_ARG;
+  if ((int)pl->st.size() >= kMaxStreams) return VFRB_ERR_NOMEM;
+  if (cudaSetDevice(pl->P.device) != cudaSuccess) return VFRB_ERR_CUDA;
+  // admission: the new stream's device bytes must fit the budget beside the
+  // streams already open (the caller retries once others have closed)
+  const int64_t need = stream_bytes(pl, pl->ring_frames, pl->R1, pl->R2);
+  const int64_t used = vfrb_plan_device_bytes(pl);
+  size_t fr = 0, tot = 0;
+  if (cudaMemGetInfo(&fr, &tot) != cudaSuccess) return VFRB_ERR_CUDA;
+  const int64_t budget = pl->P.device_bytes > 0 ? pl->P.device_bytes : used + (int64_t)(0.9 * (double)fr);
+  if (used + need > budget) return VFRB_ERR_NOMEM;
+  const int id = (int)pl->st.size();
+  int st = create_stream(pl, id, pl->ring_frames, pl->R1, pl->R2);
+  StreamSt* s = pl->st.back().get();
+  if (st == VFRB_OK &&
+      (cudaStreamSynchronize(s->cs) != cudaSuccess || cudaStreamSynchronize(s->xs) != cudaSuccess))
+    st = VFRB_ERR_CUDA;
+  if (st != VFRB_OK) {
+    s->res.release();
+    pl->st.pop_back();
+    return st;
+  }
+  *stream = id;
+  return VFRB_OK;
+}
+
+int vfrb_stream_close(vfrb_plan* pl, int stream) {
+  if (!pl || stream < 0 || stream >= (int)pl->st.size() || !pl->st[stream]) return VFRB_ERR_ARG;
+  StreamSt* s = pl->st[stream].get();
+  if (!s->ended) vfrb_push_frames(pl, stream, nullptr, 0);  // end of data; a reader error closes all the same
+  for (const ResultSlot* r : pl->queue)
+    if (r->r.stream == stream) return VFRB_PENDING;  // results still to be polled
+  if (pl->held && pl->held->r.stream == stream) {  // the last poll's result of this stream ends here
+    pl->held->state = 0;
+    pl->held = nullptr;
+  }
+  s->res.release();
+  pl->st[stream].reset();
+  return VFRB_OK;
+}
 
 int vfrb_push_frames(vfrb_plan* pl, int stream, const uint8_t* bytes, size_t nbytes) {
-  if (!pl || stream < 0 || stream >= (int)pl->st.size()) return VFRB_ERR_ARG;
+  if (!pl || stream < 0 || stream >= (int)pl->st.size() || !pl->st[stream]) return VFRB_ERR_ARG;
   StreamSt* s = pl->st[stream].get();
   if (s->ended) return VFRB_ERR_ARG;
   if (s->reader_error) return s->reader_error;
@@ -1165,7 +1242,7 @@ int vfrb_poll(vfrb_plan* pl, vfrb_result* out, int wait) {
   }
   if (pl->queue.empty()) {
     for (auto& s : pl->st)
-      if (!s->ended) return VFRB_PENDING;
+      if (s && !s->ended && !s->reader_error) return VFRB_PENDING;  // a failed stream produces nothing more
     return VFRB_EOD;
   }
   auto it = pl->queue.begin();
@@ -1222,13 +1299,13 @@ int vfrb_poll(vfrb_plan* pl, vfrb_result* out, int wait) {
 }
 
 const char* vfrb_stream_log(vfrb_plan* pl, int stream) {
-  if (!pl || stream < 0 || stream >= (int)pl->st.size()) return "";
+  if (!pl || stream < 0 || stream >= (int)pl->st.size() || !pl->st[stream]) return "";
   pl->logtmp = pl->st[stream]->logtext;
   return pl->logtmp.c_str();
 }
 
 int vfrb_stream_tstart(vfrb_plan* pl, int stream, double* mjd) {
-  if (!pl || !mjd || stream < 0 || stream >= (int)pl->st.size()) return VFRB_ERR_ARG;
+  if (!pl || !mjd || stream < 0 || stream >= (int)pl->st.size() || !pl->st[stream]) return VFRB_ERR_ARG;
   const StreamSt* s = pl->st[stream].get();
   if (s->started) {
     *mjd = s->tstart_mjd;
