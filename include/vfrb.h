@@ -351,7 +351,8 @@ void vfrb_params_default(vfrb_params* p);
 typedef struct vfrb_cand {
   int32_t dm_index;
   int32_t width;                   /* boxcar width in samples (1 = none)     */
-  int64_t t;                       /* absolute FB row of the peak            */
+  int64_t t;                       /* absolute FB row of the peak (with the
+                                    * boxcar search: of the box's first row) */
   float snr;
   float dm;
 } vfrb_cand;
