@@ -5,7 +5,8 @@ Tolerances (stated here, used below):
     row) for every element -- FP32 FFT error is spread evenly over the bins, so
     per-element relative error is only meaningful for non-tiny bins; the
     per-element relative error of bins above 10% of the row mean is also
-    checked at NAVE >= 4;
+    checked at NAVE >= 4; for tones and impulses (power in a few bins) the
+    bound is 1e-5 of the row's peak;
   * bandpass output: |gpu - oracle| <= 1e-6 * max|input| (one float rounding);
   * dedispersed series (FP32): max |gpu - oracle| <= 1e-5 * rms(oracle series);
   * per-DM ave/sigma: relative <= 1e-5; peak: relative <= 1e-4; FRB flag exact;
@@ -75,8 +76,8 @@ def test_channelise_tones_and_impulses(vf, O):
     """Known inputs through the 12500-point transform (nave 1, full band):
     an on-bin tone in pol 0 only, an off-bin tone in pol 1 only (leakage),
     one impulse per pol (flat spectrum) and both tones over noise.  Against
-    the FP64 oracle, plus the spectra's own structure: the tone's channel,
-    the flat impulse spectrum."""
+    the FP64 oracle within 1e-5 of each row's peak, plus the spectra's own
+    structure: the tone's channel, the flat impulse spectrum."""
     torch = _torch()
     n = 12500
     t = np.arange(n)
@@ -99,7 +100,11 @@ def test_channelise_tones_and_impulses(vf, O):
     ns = len(p0) // 5000
     s0 = torch.arange(ns, dtype=torch.int64, device=dev) * 5000
     got = vf.channelise(d, s0, s0 + len(p0), 0, 4, L).cpu().numpy().astype(np.float64)
-    _assert_fb_close(got, ref)
+    # a tone puts its power in one or two bins: FP32 transform errors scale
+    # with the row's peak, not its mean
+    e = np.max(np.abs(got - ref) / ref.max(axis=1, keepdims=True), axis=1)
+    print("tones/impulses max err / row peak", e)
+    assert e.max() <= 1e-5
     assert int(np.argmax(got[0])) == 1000 - L.nskip  # the on-bin tone's channel
     assert got[0, 1000 - L.nskip] > 1e4 * np.median(got[0])
     pk = int(np.argmax(got[1])) + L.nskip  # off-bin: the power sits in bins 3001 and 3002
