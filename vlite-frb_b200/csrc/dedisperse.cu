@@ -416,6 +416,10 @@ struct RegGroup {
   unsigned* d_gpack = nullptr;
   int* d_bmin = nullptr;
   int bmin_mid_max = 0;             // max over CTA blocks of bmin at the middle channel
+  // the same three for CTAs of 16 warps (16*D trials), used by the pattern kernel's
+  // one-CTA-per-SM form
+  int nblocks16 = 0, span_16w = 0, bmin_mid_max16 = 0;
+  int* d_bmin16 = nullptr;
   unsigned char* d_gpat = nullptr;  // pattern id per (group, channel), D = 4 and 2
   long long n_generic = 0;          // (group, channel) pairs outside the pattern table
 };
@@ -545,17 +549,25 @@ static int reg_launch(const vfrb_ddplan* pl, int v, const vfrb_dd_args& a, DmPar
   return VFRB_OK;
 }
 
-template <typename T, int D, int TT, int SMAX>
+template <typename T, int D, int TT, int SMAX, int W>
 static int pat_launch_t(const vfrb_ddplan* pl, const RegGroup& g, const vfrb_dd_args& a, DmPartial* part,
                         float out_scale, cudaStream_t s, int* ntb) {
   constexpr int VEC = 16 / (int)sizeof(T);
   constexpr int NT = 32 * TT;
   *ntb = 0;
   if (g.D != D || g.smax > SMAX || !g.d_gpat) return VFRB_OK;  // not applicable
-  const int lm = (g.span + VEC - 1 + NT + SMAX + VEC - 1) / VEC * VEC;
-  // two CTAs per SM: keep each under ~110 KB of shared memory
-  const int per_ch = 2 * lm * (int)sizeof(T) + 3 * kPatWarps * 4;
-  const int chunk = std::min(32, (110 * 1024 - kPatWarps * 4 - 32) / per_ch);
+  // CTA blocks of W*D trials: the 8-warp tables, or the 16-warp ones
+  const int span = W == 16 ? g.span_16w : g.span;
+  const int nblocks = W == 16 ? g.nblocks16 : g.nblocks;
+  const int* bmin = W == 16 ? g.d_bmin16 : g.d_bmin;
+  const int mid_max = W == 16 ? g.bmin_mid_max16 : g.bmin_mid_max;
+  if (!bmin) return VFRB_OK;
+  const int lm = (span + VEC - 1 + NT + SMAX + VEC - 1) / VEC * VEC;
+  // 8 warps: two CTAs per SM, each under ~110 KB of shared memory; 16 warps:
+  // one CTA per SM with ~220 KB
+  const int budget = (W == 16 ? 220 : 110) * 1024;
+  const int per_ch = 2 * lm * (int)sizeof(T) + 3 * W * 4;
+  const int chunk = std::min(32, (budget - W * 4 - 32) / per_ch);
   if (chunk < 4) return VFRB_OK;
   DdPatParams k{};
   k.fb = a.fb;
@@ -574,22 +586,22 @@ static int pat_launch_t(const vfrb_ddplan* pl, const RegGroup& g, const vfrb_dd_
   k.gbase = g.d_gbase;
   k.gpack = g.d_gpack;
   k.gpat = g.d_gpat;
-  k.bmin = g.d_bmin;
+  k.bmin = bmin;
   k.chunk = chunk;
   k.lmax = lm;
   k.err = a.d_err;
-  const size_t meta = 16 + ((size_t)3 * kPatWarps * chunk + kPatWarps + 3) / 4 * 16;
+  const size_t meta = 16 + ((size_t)3 * W * chunk + W + 3) / 4 * 16;
   const size_t smem = meta + (size_t)2 * chunk * lm * sizeof(T);
   cudaError_t e =
-      cudaFuncSetAttribute(k_dedisp_pat<T, D, TT, SMAX>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      cudaFuncSetAttribute(k_dedisp_pat<T, D, TT, SMAX, W>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return VFRB_ERR_CUDA;
   const long long ntime = (a.nt_out + NT - 1) / NT;
   // grid y runs time blocks shifted by each DM block's delay at the middle
   // channel (see the kernel); the first and last rows hold empty CTAs
-  const long long ny = ntime + g.bmin_mid_max / NT;
+  const long long ny = ntime + mid_max / NT;
   if (ny > 65535) return VFRB_OK;
-  dim3 grid((unsigned)g.nblocks, (unsigned)ny);
-  k_dedisp_pat<T, D, TT, SMAX><<<grid, kPatWarps * 32, smem, s>>>(k);
+  dim3 grid((unsigned)nblocks, (unsigned)ny);
+  k_dedisp_pat<T, D, TT, SMAX, W><<<grid, W * 32, smem, s>>>(k);
   const int st = cuda_status(cudaGetLastError());
   if (st == VFRB_OK) *ntb = (int)ntime;
   return st;
@@ -605,14 +617,18 @@ static int pat_launch(const vfrb_ddplan* pl, int v, const vfrb_dd_args& a, DmPar
   if (!g) return VFRB_OK;
   if (a.storage == VFRB_F32) {
     if (a.chan_stride % 4 || ((unsigned long long)a.row_mask + 1ULL) % 4) return VFRB_OK;
-    if (D == 4) return pat_launch_t<float, 4, 15, VFRB_PAT4_SMAX>(pl, *g, a, part, 1.f, s, ntb);
-    return pat_launch_t<float, 2, 27, VFRB_PAT2_SMAX>(pl, *g, a, part, 1.f, s, ntb);
+    // FP32, four trials: 16-warp CTAs (one per SM) share each staged row
+    // between twice as many trials (48.9 vs 55.2 ms at the 61,440-sample x
+    // 2048-trial shape); FP16 tiles are half the size, and there the 8-warp
+    // form is faster (47.7 vs 49.3 ms)
+    if (D == 4) return pat_launch_t<float, 4, 15, VFRB_PAT4_SMAX, 16>(pl, *g, a, part, 1.f, s, ntb);
+    return pat_launch_t<float, 2, 27, VFRB_PAT2_SMAX, 8>(pl, *g, a, part, 1.f, s, ntb);
   }
   if (a.storage == VFRB_F16) {
     if (a.chan_scale || !(a.uniform_scale > 0.f)) return VFRB_OK;
     if (a.chan_stride % 8 || ((unsigned long long)a.row_mask + 1ULL) % 8) return VFRB_OK;
-    if (D == 4) return pat_launch_t<__half, 4, 14, VFRB_PAT4_SMAX>(pl, *g, a, part, a.uniform_scale, s, ntb);
-    return pat_launch_t<__half, 2, 26, VFRB_PAT2_SMAX>(pl, *g, a, part, a.uniform_scale, s, ntb);
+    if (D == 4) return pat_launch_t<__half, 4, 14, VFRB_PAT4_SMAX, 8>(pl, *g, a, part, a.uniform_scale, s, ntb);
+    return pat_launch_t<__half, 2, 26, VFRB_PAT2_SMAX, 8>(pl, *g, a, part, a.uniform_scale, s, ntb);
   }
   return VFRB_OK;
 }
@@ -869,6 +885,22 @@ static int build_group(vfrb_ddplan* p, const int32_t* h_off, int D, int smax_all
       bm[(size_t)b * nchan + c] = mn;
       span = std::max(span, mx - mn);
     }
+  // the same per-block table for 16-warp CTAs (the pattern kernel's
+  // one-CTA-per-SM form)
+  const int DB16 = 16 * D;
+  const int nb16 = (ndm + DB16 - 1) / DB16;
+  std::vector<int> bm16((size_t)nb16 * nchan);
+  int span16 = 0;
+  for (int b = 0; b < nb16; ++b)
+    for (int c = 0; c < nchan; ++c) {
+      int mn = 0x7fffffff, mx = 0;
+      for (int d = b * DB16; d < std::min(ndm, (b + 1) * DB16); ++d) {
+        mn = std::min(mn, off(d, c));
+        mx = std::max(mx, off(d, c));
+      }
+      bm16[(size_t)b * nchan + c] = mn;
+      span16 = std::max(span16, mx - mn);
+    }
   RegGroup* slot = nullptr;
   for (auto& r : p->reg)
     if (r.D == 0) {
@@ -883,6 +915,9 @@ static int build_group(vfrb_ddplan* p, const int32_t* h_off, int D, int smax_all
   for (int b = 0; b < nb; ++b) g.bmin_mid_max = std::max(g.bmin_mid_max, bm[(size_t)b * nchan + nchan / 2]);
   g.ngroups = ng;
   g.nblocks = nb;
+  g.nblocks16 = nb16;
+  g.span_16w = span16;
+  for (int b = 0; b < nb16; ++b) g.bmin_mid_max16 = std::max(g.bmin_mid_max16, bm16[(size_t)b * nchan + nchan / 2]);
   const bool with_pat = (D == 4 && smax <= VFRB_PAT4_SMAX) || (D == 2 && smax <= VFRB_PAT2_SMAX);
   std::vector<unsigned char> pt;
   if (with_pat) {
@@ -895,16 +930,19 @@ static int build_group(vfrb_ddplan* p, const int32_t* h_off, int D, int smax_all
   bool ok = cudaMalloc(&g.d_gbase, gb.size() * sizeof(int)) == cudaSuccess &&
             cudaMalloc(&g.d_gpack, gp.size() * sizeof(unsigned)) == cudaSuccess &&
             cudaMalloc(&g.d_bmin, bm.size() * sizeof(int)) == cudaSuccess &&
+            cudaMalloc(&g.d_bmin16, bm16.size() * sizeof(int)) == cudaSuccess &&
             (!with_pat || cudaMalloc(&g.d_gpat, pt.size()) == cudaSuccess);
   ok = ok && cudaMemcpy(g.d_gbase, gb.data(), gb.size() * sizeof(int), cudaMemcpyHostToDevice) == cudaSuccess &&
        cudaMemcpy(g.d_gpack, gp.data(), gp.size() * sizeof(unsigned), cudaMemcpyHostToDevice) == cudaSuccess &&
        cudaMemcpy(g.d_bmin, bm.data(), bm.size() * sizeof(int), cudaMemcpyHostToDevice) == cudaSuccess &&
+       cudaMemcpy(g.d_bmin16, bm16.data(), bm16.size() * sizeof(int), cudaMemcpyHostToDevice) == cudaSuccess &&
        (!with_pat || cudaMemcpy(g.d_gpat, pt.data(), pt.size(), cudaMemcpyHostToDevice) == cudaSuccess);
   if (!ok) {
     cudaGetLastError();
     cudaFree(g.d_gbase);
     cudaFree(g.d_gpack);
     cudaFree(g.d_bmin);
+    cudaFree(g.d_bmin16);
     cudaFree(g.d_gpat);
     return VFRB_ERR_NOMEM;
   }
@@ -919,6 +957,7 @@ int ddplan_destroy(vfrb_ddplan* p) {
     if (g.d_gbase) cudaFree(g.d_gbase);
     if (g.d_gpack) cudaFree(g.d_gpack);
     if (g.d_bmin) cudaFree(g.d_bmin);
+    if (g.d_bmin16) cudaFree(g.d_bmin16);
     if (g.d_gpat) cudaFree(g.d_gpat);
   }
   delete p;

@@ -26,7 +26,7 @@
 
 namespace vfrb {
 
-constexpr int kPatWarps = 8;
+constexpr int kPatWarps = 8;  // warps per CTA of the two-CTAs-per-SM form (the other: 16, one CTA)
 constexpr unsigned char kPatGeneric = 255;
 
 struct DdPatParams {
@@ -202,8 +202,10 @@ __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, unsigned by
                : "memory");
 }
 
-template <typename T, int D, int TT, int SMAX>
-__global__ void __launch_bounds__(kPatWarps * 32, 2) k_dedisp_pat(const DdPatParams p) {
+// W warps per CTA: 8 (two CTAs per SM, ~110 KB of tiles each) or 16 (one
+// CTA per SM sharing ~220 KB of tiles between twice as many DM trials)
+template <typename T, int D, int TT, int SMAX, int W>
+__global__ void __launch_bounds__(W * 32, 16 / W) k_dedisp_pat(const DdPatParams p) {
   constexpr int VEC = 16 / (int)sizeof(T);
   constexpr int NT = 32 * TT;
   static_assert(sizeof(T) == 4 ? (TT & 1) == 1 : (TT & 3) == 2, "lane stride must spread loads over all banks");
@@ -214,10 +216,10 @@ __global__ void __launch_bounds__(kPatWarps * 32, 2) k_dedisp_pat(const DdPatPar
   //                | tiles[2][CH][LM] (16-byte aligned)
   unsigned long long* s_full = reinterpret_cast<unsigned long long*>(smp4);
   int* s_slot = reinterpret_cast<int*>(smp4 + 1);
-  unsigned* s_pk = reinterpret_cast<unsigned*>(s_slot + kPatWarps * CH);
-  int* s_run = reinterpret_cast<int*>(s_pk + kPatWarps * CH);
-  int* s_nrun = s_run + kPatWarps * CH;
-  const int meta_q = 1 + (3 * kPatWarps * CH + kPatWarps + 3) / 4;
+  unsigned* s_pk = reinterpret_cast<unsigned*>(s_slot + W * CH);
+  int* s_run = reinterpret_cast<int*>(s_pk + W * CH);
+  int* s_nrun = s_run + W * CH;
+  const int meta_q = 1 + (3 * W * CH + W + 3) / 4;
   int4* tiles = smp4 + meta_q;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   // DM blocks run along x (fastest); along y, DM block b takes time block
@@ -230,27 +232,27 @@ __global__ void __launch_bounds__(kPatWarps * 32, 2) k_dedisp_pat(const DdPatPar
   const int tb = (int)blockIdx.y - __ldg(p.bmin + (long long)blk * p.nchan + p.nchan / 2) / NT;
   if (tb < 0 || (long long)tb * NT >= p.nt_out) return;
   const long long t0 = (long long)tb * NT;
-  const int g = min(blk * kPatWarps + warp, p.ngroups - 1);
+  const int g = min(blk * W + warp, p.ngroups - 1);
   const T* fb = reinterpret_cast<const T*>(p.fb);
   const int nchunks = (p.nchan + CH - 1) / CH;
   const long long vend = p.row0 + p.nrows_valid;
   const unsigned long long rmask = (unsigned long long)p.row_mask;
   int err = 0;
   if (tid == 0) {
-    mbar_init(&s_full[0], kPatWarps);
-    mbar_init(&s_full[1], kPatWarps);
+    mbar_init(&s_full[0], W);
+    mbar_init(&s_full[1], W);
     mbar_fence_init();
   }
   __syncthreads();
 
-  // Staging, shared by the eight warps: warp w copies its ceil(CH/8)
+  // Staging, shared by the W warps: warp w copies its ceil(CH/W)
   // channels of chunk k into tile buffer b.  A channel's rows [a, a + LM) go
   // in one bulk asynchronous copy when they are all valid (two when they
   // wrap the ring: the split is at the ring end, a multiple of 16 bytes);
   // otherwise the warp copies them itself, with zeros outside
   // [0, row0 + nrows_valid), before announcing its bulk bytes.  Each warp
-  // arrives once per buffer phase, so the barrier counts eight arrivals.
-  const int per = (CH + kPatWarps - 1) / kPatWarps;
+  // arrives once per buffer phase, so the barrier counts W arrivals.
+  const int per = (CH + W - 1) / W;
   // bmin of this lane's staging channel of chunk k (loaded ahead of use)
   auto stage_bmin = [&](int k) -> int {
     if (k >= nchunks) return 0;
@@ -409,7 +411,7 @@ __global__ void __launch_bounds__(kPatWarps * 32, 2) k_dedisp_pat(const DdPatPar
   const float fs = p.out_scale / (float)p.nchan;
   const bool plain = p.out_scale == 1.f;
   const float fn = (float)p.nchan;
-  const int gw = blk * kPatWarps + warp;
+  const int gw = blk * W + warp;
 #pragma unroll
   for (int j = 0; j < D; ++j) {
     const int d = gw * D + j;
