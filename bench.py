@@ -557,9 +557,12 @@ def main():
     del frames
     torch.cuda.empty_cache()
     e2e = run_e2e(vf, host, 0, args.e2e_steps)
+    e2e16 = run_e2e(vf, host, 1, args.e2e_steps) if not args.skip_extras else None
     del host
     e2e_s = dist_max(dist, e2e["s_per_step"])
     e2e_rtf = world * data_s / e2e_s
+    # every rank takes the same collectives: the FP16 leg runs on all or none
+    e2e16_s = dist_max(dist, e2e16["s_per_step"]) if e2e16 is not None else None
     lat = np.array(e2e["lat"]) if e2e["lat"] else np.array([float("nan")])
     if rank != 0:
         return 0
@@ -628,6 +631,9 @@ def main():
                         "stages_ms_per_step": f16["stage_ms"], "speedup_vs_f32": f32["ms"] / f16["ms"],
                         "dedisperse_speedup_vs_f32": f32["stage_ms"][2] / f16["stage_ms"][2],
                         "autotune_ms": {"variant": f16["variant"], "times": {str(k): v for k, v in f16["tune"].items()}}}
+        if e2e16_s is not None:  # through the plan API as well (PCIe-bound like the FP32 figure)
+            line["fp16"]["e2e"] = {"value": world * data_s / e2e16_s, "unit": "s data/s",
+                                   "h2d_bytes_per_step": int(e2e16["h2d"]), "d2h_bytes_per_step": int(e2e16["d2h"])}
     if not args.skip_extras:
         try:
             line["cpu_baseline"] = {k: v for k, v in cpu_baseline(args.cpu_sample).items() if k != "seconds"}
