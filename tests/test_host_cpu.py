@@ -164,3 +164,21 @@ def test_cluster_cands_matches_oracle(vf, O, seed):
         ocl, olab = O.cluster_cands(tup, dm_tol, t_tol)
         assert [(x["dm_index"], x["t"], x["width"], x["snr"]) for x in cl] == ocl
         assert list(lab) == olab
+
+
+def test_cluster_cands_in_place(vf):
+    """The output array may be the input array (clusters written in place)."""
+    import ctypes as C
+    rng = np.random.default_rng(11)
+    n = 200
+    arr = (vf.Cand * n)()
+    for i in range(n):
+        arr[i] = vf.Cand(dm_index=int(rng.integers(0, 40)), width=int(2 ** rng.integers(0, 4)),
+                         t=int(rng.integers(0, 3000)), snr=float(rng.integers(60, 90) / 8.0), dm=0.0)
+    cands = [dict(dm_index=a.dm_index, width=a.width, t=a.t, snr=a.snr) for a in arr]
+    want, _ = vf.cluster_cands(cands, dm_tol=3, t_tol=20)
+    nout = C.c_int32(0)
+    lib = vf.lib()
+    assert lib.vfrb_cluster_cands(arr, n, 3, 20, arr, C.byref(nout), None) == 0
+    got = [dict(dm_index=a.dm_index, width=a.width, t=a.t, snr=a.snr, dm=a.dm) for a in arr[:nout.value]]
+    assert got == want
