@@ -20,7 +20,8 @@ def build():
         subprocess.run(["gcc", "-O3", "-march=x86-64-v3", "-fopenmp", "-fPIC", "-shared", f"-DREAL={real}",
                         "-o", so, src, "-lm"], check=True)
     ref = os.path.join(HERE, "build_ref.py")
-    if os.path.exists(ref) and os.path.isdir("/root/reference"):
+    refdir = os.environ.get("VFRB_REFERENCE_DIR") or os.path.join(os.path.dirname(os.path.dirname(HERE)), "reference")
+    if os.path.exists(ref) and os.path.isdir(refdir):
         subprocess.run([sys.executable, ref], check=False)
 
 

@@ -24,7 +24,8 @@ import sys
 import tempfile
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-REF = os.environ.get("VFRB_REFERENCE_DIR", "/root/reference")
+# the reference checkout: $VFRB_REFERENCE_DIR, else "reference" beside this repository
+REF = os.environ.get("VFRB_REFERENCE_DIR") or os.path.join(os.path.dirname(os.path.dirname(HERE)), "reference")
 OUT = os.path.join(HERE, "_ref")
 NVCC = "/usr/local/cuda/bin/nvcc"
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]

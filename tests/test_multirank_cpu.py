@@ -104,3 +104,23 @@ def test_reference_arm_line_contract():
     cb = d["cpu_baseline"]
     assert cb["kind"] in ("port", "reference") and cb["cores"] >= 1 and cb["value"] == d["value"] and cb["sample"]
     assert d["e2e"] == {"value": d["value"], "unit": "s data/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}
+    # the same workload object as the GPU arm; ms_per_step is the time of the
+    # sample a step really ran (value = sample seconds / step seconds)
+    sys.path.insert(0, ROOT)
+    import bench
+    assert d["config"] == bench.bench_config(bench.DURATION, 1)
+    assert abs(d["ms_per_step"] / 1000.0 * d["value"] - 0.05) < 1e-6
+
+
+def test_reference_arm_maps_no_product_library():
+    """The reference arm's process loads the oracle's port and nothing of the
+    product: libvfrb.so is never mapped."""
+    import subprocess
+    import sys
+    code = ("import sys, runpy; sys.argv = ['bench.py', '--impl', 'reference', '--steps', '1', '--warmup', '1', "
+            "'--cpu-sample', '0.05']; import bench; bench.main(); "
+            "maps = open('/proc/self/maps').read(); print('LIBVFRB' if 'libvfrb' in maps else 'CLEAN'); "
+            "print('ORACLE' if 'liboracle32' in maps else 'NO-ORACLE')")
+    r = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, timeout=600, cwd=ROOT)
+    assert r.returncode == 0, r.stderr[-2000:]
+    assert "CLEAN" in r.stdout and "ORACLE" in r.stdout, r.stdout[-500:]

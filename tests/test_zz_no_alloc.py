@@ -3,7 +3,9 @@
 Both entry points are called through the C ABI on the same inputs; the
 no-alloc call gets no workspace at all.  Two different cases run back to
 back through the shared scratch, so stale partial sums from the first call
-would show in the second call's statistics.
+would show in the second call's statistics; the first case and the size
+limit run once per dedispersion kernel variant, since each variant writes
+the partial sums with its own time blocking.
 """
 import ctypes as C
 
@@ -68,20 +70,27 @@ def _compare(got, want):
         assert np.array_equal(st_g[k].cpu().numpy(), st_w[k].cpu().numpy()), k
 
 
+# every kernel variant writes the partial sums with its own time blocking;
+# a variant that does not apply to a plan runs the staged kernel instead
+VARIANTS = list(range(1, 8))  # VFRB_DD_STAGED .. VFRB_DD_PAT2
+
+
 def test_noalloc_matches_dedisperse_two_calls(vf, O):
     import torch
     lib = _bind(vf)
     assert lib.vfrb_dedisperse_noalloc_scratch_bytes() == 4 << 20
-    cases = [(1, 96, 256, 3000, 120.0), (2, 40, 192, 700, 60.0)]
-    for seed, ndm, nch, nt, dm_max in cases:
+    cases = [(1, 96, 256, 3000, 120.0, VARIANTS), (2, 40, 192, 700, 60.0, [0])]
+    for seed, ndm, nch, nt, dm_max, variants in cases:
         off, fb = _filterbank(torch, O, seed, ndm, nch, nt, dm_max)
         plan = vf.DedispPlan(off)
         ws = torch.empty(plan.workspace_bytes(nt), dtype=torch.uint8, device="cuda")
-        st_w, *want = _run(vf, lib, lib.vfrb_dedisperse, plan, fb, nt, ws)
-        st_g, *got = _run(vf, lib, lib.vfrb_dedisperse_noalloc, plan, fb, nt, None)
-        assert st_w == 0 and st_g == 0
-        _compare(got, want)
-        assert int(got[1]["frb"][ndm // 3]) == 1
+        for v in variants:
+            plan.set_variant(vf.F32, v)
+            st_w, *want = _run(vf, lib, lib.vfrb_dedisperse, plan, fb, nt, ws)
+            st_g, *got = _run(vf, lib, lib.vfrb_dedisperse_noalloc, plan, fb, nt, None)
+            assert st_w == 0 and st_g == 0, v
+            _compare(got, want)
+            assert int(got[1]["frb"][ndm // 3]) == 1, v
 
 
 def test_noalloc_size_limit(vf, O):
@@ -98,11 +107,14 @@ def test_noalloc_size_limit(vf, O):
     assert plan.workspace_bytes(nt) <= limit
     fb = torch.from_numpy(rng.standard_normal((nch, nt + 256)).astype(np.float32)).cuda()
     ws = torch.empty(plan.workspace_bytes(nt), dtype=torch.uint8, device="cuda")
-    st_w, *want = _run(vf, lib, lib.vfrb_dedisperse, plan, fb, nt, ws)
-    st_g, *got = _run(vf, lib, lib.vfrb_dedisperse_noalloc, plan, fb, nt, None)
-    assert st_w == 0 and st_g == 0
-    _compare(got, want)
-    del want, got, ws
+    for v in VARIANTS:
+        plan.set_variant(vf.F32, v)
+        st_w, *want = _run(vf, lib, lib.vfrb_dedisperse, plan, fb, nt, ws)
+        st_g, *got = _run(vf, lib, lib.vfrb_dedisperse_noalloc, plan, fb, nt, None)
+        assert st_w == 0 and st_g == 0, v
+        _compare(got, want)
+        del want, got
+    del ws
     nt2 = nt + 256
     assert plan.workspace_bytes(nt2) > limit
     st_r, out_r, _ = _run(vf, lib, lib.vfrb_dedisperse_noalloc, plan, fb, nt2, None)

@@ -35,24 +35,55 @@ static __device__ __align__(256) unsigned char g_dd_scratch[kScratchBytes];
 
 constexpr int kMaxDevices = 64;
 std::mutex g_setup_mu;
-void* g_scratch_ptr[kMaxDevices] = {};
+struct ScratchEntry {
+  void* ctx;  // CUDA context the address belongs to
+  void* ptr;
+};
+ScratchEntry g_scratch[kMaxDevices] = {};
 
-// Device address of g_dd_scratch on the current device, looked up once per
-// device (the first call on a device may load the module, so make that call
-// before any stream capture).
+// cuCtxGetCurrent through the runtime's driver entry point (no link against
+// libcuda); null when the driver does not offer it.
+using CtxGetCurrentFn = int (*)(void**);
+CtxGetCurrentFn ctx_get_current() {
+  static CtxGetCurrentFn fn = [] {
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess) {
+      cudaGetLastError();
+      return (CtxGetCurrentFn) nullptr;
+    }
+    return reinterpret_cast<CtxGetCurrentFn>(f);
+  }();
+  return fn;
+}
+
+// Device address of g_dd_scratch in the current device's current context.
+// It is looked up once per device and context (the lookup may load the
+// module, so make the first call on a device before any stream capture) and
+// looked up again when the device's context changes (another context made
+// current, or the primary context re-created after cudaDeviceReset).
 int scratch_for_current_device(void** out) {
   int dev = -1;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return VFRB_ERR_CUDA;
   if (dev < 0 || dev >= kMaxDevices) return VFRB_ERR_UNSUPPORTED;
+  // Before the runtime has bound a context to this thread there is none to
+  // key on; the address is then looked up (which binds the primary context)
+  // and keyed on the next call.
+  void* ctx = nullptr;
+  CtxGetCurrentFn cur = ctx_get_current();
+  const bool have_ctx = cur && cur(&ctx) == 0 && ctx;
   std::lock_guard<std::mutex> lk(g_setup_mu);
-  if (!g_scratch_ptr[dev]) {
+  ScratchEntry& ent = g_scratch[dev];
+  if (!have_ctx || !ent.ptr || ent.ctx != ctx) {
     void* p = nullptr;
     e = cudaGetSymbolAddress(&p, g_dd_scratch);
     if (e != cudaSuccess || !p) return VFRB_ERR_CUDA;
-    g_scratch_ptr[dev] = p;
+    ent.ptr = p;
+    ent.ctx = have_ctx ? ctx : nullptr;
   }
-  *out = g_scratch_ptr[dev];
+  *out = ent.ptr;
   return VFRB_OK;
 }
 
