@@ -53,13 +53,25 @@ def load_pkg():
     return m
 
 
-def pulses(seed=SEED, n=20, duration=DURATION):
-    rng = np.random.default_rng(seed + 7)
-    out = []
-    for _ in range(n):
-        dm = float(rng.uniform(50, DM_MAX))
-        out.append((float(rng.uniform(0.2, duration - 0.5)), dm, float(rng.uniform(1, 10)), float(rng.uniform(8, 30))))
-    return out
+def load_synth():
+    """The synthetic-input generator on its own, without the package (whose
+    import maps libvfrb.so): the reference arm and the CPU baseline use it
+    for their inputs and nothing else."""
+    if "vfrb_synth_only" in sys.modules:
+        return sys.modules["vfrb_synth_only"]
+    spec = importlib.util.spec_from_file_location("vfrb_synth_only", os.path.join(PKG_DIR, "synth.py"))
+    m = importlib.util.module_from_spec(spec)
+    sys.modules["vfrb_synth_only"] = m
+    spec.loader.exec_module(m)
+    return m
+
+
+def bench_config(duration, world):
+    """The workload's `config` object, shared by both arms of the bench."""
+    return {"workload": WORKLOAD, "seconds_per_step": duration, "nchan": 6250, "ndm": NDM, "nave": NAVE,
+            "form": "plain FP32", "inputs_larger_than_l2": True,
+            "l2_note": "inputs (15.5 GB of VDIF per step) exceed the 126 MB L2; no flush needed",
+            "parallelism": f"streams x{world} (one independent stream per GPU)"}
 
 
 def dm_grid():
@@ -274,14 +286,15 @@ _CPU_CACHE = {}
 
 def run_serving(vf, storage, nstreams=16, paced_s=15.0, load=1.5, seed0=100):
     """The serving configuration: nstreams independent streams (seeds 100..,
-    one dispersed pulse each) whose bytes arrive in chunks of U(0.5, 2.0) s
+    one dispersed pulse each) whose bytes arrive in chunks of U(0.5, 8.0) s
     (cut anywhere, not frame-aligned).  Each stream's frames are generated on
-    the device as its chunks are needed (headers continue across chunks).
-    First every stream is filled past the 12.4-s DM-1000 overlap back to
-    back; then, for paced_s seconds, chunks arrive as one Poisson process
-    totalling `load` x real time and results are polled as they complete.
-    Returns the chunk latencies of that phase (data pushed -> result on the
-    host) and every candidate."""
+    the device as its chunks are needed (headers continue across chunks) and
+    pushed from page-locked host memory.  First every stream is filled back
+    to back past its pulse's output chunk plus the 12.4-s DM-1000 overlap,
+    so every pulse is searched; then, for paced_s seconds, chunks arrive as
+    one Poisson process totalling `load` x real time and results are polled
+    as they complete.  Returns the chunk latencies of that phase (data pushed
+    -> result on the host) and every candidate."""
     import torch
     from vlite_frb_b200 import synth
     fps, pair = 25600, 2 * 5032
@@ -291,8 +304,9 @@ def run_serving(vf, storage, nstreams=16, paced_s=15.0, load=1.5, seed0=100):
                    outputs=vf.OUT_DMSTATS | vf.OUT_CANDS, cand_snr=7.0)
     sid = []
     tchan = NAVE * 12500 / 128e6
-    fill_s = (plan.max_delay + 1024) * tchan + 0.1
-    buf = torch.empty(int(2.0 * fps + 2) * pair, dtype=torch.uint8, pin_memory=True)
+    # the last pulse (t0 = 2.1 s) sits in output chunk 2 (rows 2048-3071)
+    fill_s = (plan.max_delay + 3 * 1024) * tchan + 0.1
+    buf = torch.empty(int(8.0 * fps + 2) * pair, dtype=torch.uint8, pin_memory=True)
     rng = np.random.default_rng(seed0)
     st = [{"pair": 0, "k": 0, "tail": torch.empty(0, dtype=torch.uint8), "sent": 0.0} for _ in range(nstreams)]
     # output sample t needs rows up to t + max_delay: pulses early in the
@@ -301,7 +315,7 @@ def run_serving(vf, storage, nstreams=16, paced_s=15.0, load=1.5, seed0=100):
 
     def push_chunk(i):
         s = st[i]
-        nbytes = int(rng.uniform(0.5, 2.0) * fps * pair)
+        nbytes = int(rng.uniform(0.5, 8.0) * fps * pair)
         nt = s["tail"].numel()
         buf[:nt] = s["tail"]
         npairs = max(0, -(-(nbytes - nt) // pair))
@@ -360,17 +374,84 @@ def run_serving(vf, storage, nstreams=16, paced_s=15.0, load=1.5, seed0=100):
                 data_s=sum(s["sent"] for s in st))
 
 
-def cpu_baseline(sample_s=1.0):
+def run_capacity(vf, storage, nstreams=16, seconds_per_stream=24.0, seed0=100, buf_s=4.0):
+    """Serving capacity with the input already on the GPU: nstreams streams
+    (seeds 100..), each a continuous stream built from a buf_s-second
+    device-resident buffer repeated with its VDIF seconds advanced, arrive
+    in chunks of U(0.5, 8) s of bytes (cut anywhere) in random stream order,
+    as fast as the engine takes them (vfrb_push_frames with device memory:
+    no PCIe).  Returns the aggregate real-time factor (data seconds of all
+    streams / wall seconds) and the chunk latencies."""
+    import torch
+    synth = load_synth()
+    fps, pair = 25600, 2 * 5032
+    plan = vf.Plan(dm_grid(), nave=NAVE, muoslowfreq=384.0, mode=vf.MODE_STREAM, storage=storage,
+                   chunk_seconds=1.0, ring_seconds=2.0, nstreams=0, outputs=vf.OUT_DMSTATS | vf.OUT_CANDS,
+                   cand_snr=7.0)
+    sid = [plan.open_stream() for _ in range(nstreams)]
+    if any(k is None for k in sid):
+        raise RuntimeError("capacity leg: streams not admitted")
+    bufs = [synth.make_vdif(synth.StreamSpec(duration=buf_s, seed=seed0 + i), device="cuda") for i in range(nstreams)]
+    nb = bufs[0].numel()
+    words = [b.view(torch.int32).view(-1, 1258) for b in bufs]  # word 0 of each frame: seconds (30 bits)
+    sec0 = [w[:, 0].clone() for w in words]
+    rng = np.random.default_rng(seed0)
+    total = int(seconds_per_stream * fps) * pair
+    pos = [0] * nstreams
+    lat = []
+
+    def push_chunk(i, n):
+        while n > 0:
+            rep, off = divmod(pos[i], nb)
+            if off == 0:  # a new repetition: advance the seconds of every frame
+                words[i][:, 0] = sec0[i] + int(rep * buf_s)
+            take = min(n, nb - off)
+            plan.push(sid[i], bufs[i][off:off + take])
+            pos[i] += take
+            n -= take
+
+    def drain(wait=False):
+        while True:
+            r = plan.poll(wait=wait)
+            if r is None:
+                return
+            lat.append(r["latency_ms"])
+
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    live = list(range(nstreams))
+    while live:
+        i = live[int(rng.integers(len(live)))]
+        n = min(int(rng.uniform(0.5, 8.0) * fps * pair), total - pos[i])
+        push_chunk(i, n)
+        drain()
+        if pos[i] >= total:
+            plan.push(sid[i], None)
+            live.remove(i)
+    drain(wait=True)
+    torch.cuda.synchronize()
+    wall = time.perf_counter() - t0
+    for k in sid:
+        plan.close_stream(k)
+    plan.close()
+    data_s = nstreams * total / (fps * pair)
+    return dict(rtf=data_s / wall, lat=np.array(lat), data_s=data_s, wall=wall)
+
+
+def cpu_baseline(sample_s=1.0, min_cpu_s=0.0):
     """The oracle's FP32 C/OpenMP port on the host cores, on `sample_s` seconds
-    of the workload (full 2048 trials, 6250 channels)."""
+    of the workload (full 2048 trials, 6250 channels): channelise, bandpass,
+    the transpose to the channel-major layout, dedisperse and per-trial
+    statistics, all inside the timed region.  The pass repeats until at least
+    `min_cpu_s` seconds of CPU time have been measured; the figures are per
+    pass."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     if "co" not in _CPU_CACHE:
         subprocess.run([sys.executable, os.path.join(ROOT, "oracle", "build_oracle.py")], check=False,
                        capture_output=True)
         from coracle import COracle  # the CPU port is the timed baseline only
         import vfrb_oracle as O
-        load_pkg()
-        from vlite_frb_b200 import synth
+        synth = load_synth()
         co = COracle(32)
         L = O.Layout(nave=NAVE, muoslowfreq=384.0)
         off, md = O.delay_table(dm_grid(), L.fch1, L.chanbw, L.tchan, L.nchanout)
@@ -383,22 +464,29 @@ def cpu_baseline(sample_s=1.0):
         _CPU_CACHE.update(co=co, L=L, off=off, nrow_s=nrow_s, p0=p0, p1=p1, cm=cm)
     c = _CPU_CACHE
     co, L, off, nrow_s, cm = c["co"], c["L"], c["off"], c["nrow_s"], c["cm"]
-    t0 = time.perf_counter()
-    fb = co.channelise(c["p0"], c["p1"], L)[:nrow_s]
-    t1 = time.perf_counter()
-    bp = co.bandpass(fb)
-    t2 = time.perf_counter()
-    cm[:, :nrow_s] = co.transpose(bp)  # the rows past the sample stand in for the carried overlap
-    t3 = time.perf_counter()
-    dd = co.dedisperse_cm(cm, off, nrow_s)
-    co.calcstats_dm(dd)
-    t4 = time.perf_counter()
-    secs = (t1 - t0) + (t2 - t1) + (t4 - t3)
+    tot = np.zeros(4)
+    npass = 0
+    while npass == 0 or tot.sum() < min_cpu_s:
+        t0 = time.perf_counter()
+        fb = co.channelise(c["p0"], c["p1"], L)[:nrow_s]
+        t1 = time.perf_counter()
+        bp = co.bandpass(fb)
+        t2 = time.perf_counter()
+        cm[:, :nrow_s] = co.transpose(bp)  # the rows past the sample stand in for the carried overlap
+        t3 = time.perf_counter()
+        dd = co.dedisperse_cm(cm, off, nrow_s)
+        co.calcstats_dm(dd)
+        t4 = time.perf_counter()
+        tot += (t1 - t0, t2 - t1, t3 - t2, t4 - t3)
+        npass += 1
+    per = tot / npass
+    secs = float(per.sum())
     rtf = sample_s / secs
     return dict(value=rtf, unit="s data/s", cores=co.threads(), kind="port",
-                sample=f"{sample_s:g} s of the workload through channelise+bandpass+dedisperse(2048 trials)+stats "
-                       f"(FP32 C/OpenMP port): channelise {t1 - t0:.2f} s, bandpass {t2 - t1:.2f} s, "
-                       f"dedisperse {t4 - t3:.2f} s", seconds=secs)
+                sample=f"{sample_s:g} s of the workload per pass ({npass} passes) through channelise + bandpass + "
+                       f"transpose + dedisperse (2048 trials) + stats (FP32 C/OpenMP port of the oracle): per pass "
+                       f"channelise {per[0]:.3f} s, bandpass {per[1]:.3f} s, transpose {per[2]:.3f} s, "
+                       f"dedisperse {per[3]:.3f} s", seconds=secs)
 
 
 def gpu_reference_baseline(vf, sample_bundles=32):
@@ -408,7 +496,7 @@ def gpu_reference_baseline(vf, sample_bundles=32):
     p = os.path.join(ROOT, "oracle", "_ref", "libref_pipe.so")
     if not os.path.exists(p):
         return None
-    from vlite_frb_b200 import synth
+    synth = load_synth()
     lib = C.CDLL(p)
     vp, ci, cf = C.c_void_p, C.c_int, C.POINTER(C.c_float)
     lib.ref_gpu_channelise.argtypes = [vp, vp, ci, ci, ci, ci, ci, ci, vp, cf]
@@ -489,8 +577,14 @@ def dist_max(dist, v):
 
 
 # --------------------------------------------------------------------------- arms
-def reference_arm(args, dist):
-    if dist and dist["rank"] != 0:
+def reference_arm(args):
+    """The reference arm: the reference has no CPU implementation of the path
+    (its three tools are CUDA programs), so this times the oracle's FP32
+    C/OpenMP port on the host cores with every host thread.  Each step is one
+    pass over a bounded sample (`--cpu-sample` seconds of the workload, all
+    2048 trials and 6250 channels), and ms_per_step is that pass's time.
+    Under torchrun only rank 0 runs; the others exit at once."""
+    if int(os.environ.get("RANK", "0")) != 0:
         return 0
     K, W = args.steps, args.warmup
     vals = []
@@ -502,12 +596,12 @@ def reference_arm(args, dist):
     secs = float(np.mean(vals))
     value = args.cpu_sample / secs
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "s data/s", "n_gpus": args.gpus,
-            "steps": K, "warmup": W, "ms_per_step": secs * 1000.0 * (DURATION / args.cpu_sample),
+            "steps": K, "warmup": W, "ms_per_step": secs * 1000.0,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (seeded VLITE VDIF stand-in; no public dataset)",
-            "config": {"workload": WORKLOAD, "sample_seconds": args.cpu_sample},
+            "config": bench_config(args.duration, args.gpus),
             "cpu_baseline": {"value": value, "unit": "s data/s", "cores": base["cores"], "kind": "port",
-                             "sample": base["sample"]},
+                             "sample": f"each step: {base['sample']}"},
             "e2e": {"value": value, "unit": "s data/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
     return 0
@@ -527,9 +621,9 @@ def main():
                     help="dedispersion kernel variant for the device legs (0: the autotuner's choice)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
-    dist = dist_init(args.gpus)
     if args.impl == "reference":
-        return reference_arm(args, dist)
+        return reference_arm(args)
+    dist = dist_init(args.gpus)
     import torch
     vf = load_pkg()
     from vlite_frb_b200 import synth
@@ -538,7 +632,7 @@ def main():
     dev = torch.device("cuda")
     # each rank processes its own independent stream (antenna): weak scaling, no collective on the data path
     spec = synth.StreamSpec(duration=args.duration, seed=stream_seed(rank),
-                            pulses=[synth.Pulse(*p) for p in pulses(duration=args.duration)])
+                            pulses=synth.injected_pulses(SEED, 20, args.duration, 50.0, DM_MAX))
     t_gen = time.perf_counter()
     frames = synth.make_vdif(spec, device=dev)
     torch.cuda.synchronize()
@@ -566,7 +660,8 @@ def main():
     lat = np.array(e2e["lat"]) if e2e["lat"] else np.array([float("nan")])
     if rank != 0:
         return 0
-    # roofline of the dominant kernel (dedispersion, K3)
+    # roofline of the dominant kernel (dedispersion, K3): it is bound by the
+    # FP32 add rate (and the shared-memory reads that feed it), not by HBM
     from json import dumps
     nt, nch = f32["rows"], f32["nchan"]
     k3_ms = f32["stage_ms"][2]
@@ -580,15 +675,35 @@ def main():
         pass
     hbm = float(peaks.get("hbm_gbs", 6650.0))
     peak_src = "measured" if "hbm_gbs" in peaks else "fallback"
-    achieved = eff_bytes / (k3_ms / 1000.0) / 1e9
-    traffic = None
-    try:
+    nsm = torch.cuda.get_device_properties(torch.cuda.current_device()).multi_processor_count
+    sm_mhz = float(peaks.get("sm_max_mhz") or f32["clocks"].get("sm_max_mhz") or 1965.0)
+    fp32_peak_adds = nsm * 128 * sm_mhz * 1e6  # 128 FP32 lanes per SM
+    adds_per_s = units * nch / (k3_ms / 1000.0)
+    traffic, traffic_src = None, None
+    try:  # DRAM bytes of a 16-s ncu capture of this kernel, scaled by output samples
         tr = json.load(open(os.path.join(ROOT, "profiles", "dedisperse_traffic.json")))
-        traffic = tr.get("bytes_per_launch")
+        traffic = tr["bytes_per_launch"] * (units / float(tr["units_per_launch"]))
+        traffic_src = tr.get("source")
     except Exception:
         pass
-    adds_per_s = units * nch / (k3_ms / 1000.0)
-    fp32_peak_adds = 148 * 128 * 1.965e9
+    # K1: compulsory bytes = raw VDIF read + FP32 filterbank written
+    k1_ms = f32["stage_ms"][0]
+    k1_bytes = data_s * (2 * 25600 * 5032 + nch * (1.0 / (NAVE * 12500 / 128e6)) * 4)
+    roofline = {"bound": "fp32_add", "achieved": adds_per_s / 1e12, "peak": fp32_peak_adds / 1e12,
+                "unit": "Tadd/s", "frac": adds_per_s / fp32_peak_adds, "traffic": traffic,
+                "kernel": "dedisperse (K3)",
+                "peak_source": f"{nsm} SMs x 128 FP32 lanes x {sm_mhz:g} MHz (MEASURED_PEAKS.json has no FP32 "
+                               f"figure)",
+                "traffic_source": traffic_src,
+                "hbm_no_reuse": {"achieved_gbs": eff_bytes / (k3_ms / 1000.0) / 1e9, "peak_gbs": hbm,
+                                 "frac": eff_bytes / (k3_ms / 1000.0) / 1e9 / hbm,
+                                 "convention": "NCHANOUT*4 B per DM-trial.sample, no reuse (values > 1 = on-chip "
+                                               "reuse); peak " + peak_src},
+                "compulsory_gbs": comp_bytes / (k3_ms / 1000.0) / 1e9,
+                "k1_channelise": {"bound": "hbm", "achieved_gbs": k1_bytes / (k1_ms / 1000.0) / 1e9,
+                                  "peak_gbs": hbm, "frac": k1_bytes / (k1_ms / 1000.0) / 1e9 / hbm,
+                                  "bytes_per_step": k1_bytes,
+                                  "note": "compulsory bytes (raw VDIF in + FP32 filterbank out); peak " + peak_src}}
     line = {
         "metric": METRIC,
         "value": rtf,
@@ -602,17 +717,8 @@ def main():
         "vs_baseline": None,
         "dtype": "f32",
         "data": "synthetic (seeded VLITE VDIF stand-in generated on the device; no public dataset)",
-        "config": {"workload": WORKLOAD, "seconds_per_step": data_s, "nchan": nch, "ndm": NDM, "nave": NAVE,
-                   "form": "plain FP32", "inputs_larger_than_l2": True,
-                   "l2_note": "inputs (15.5 GB of VDIF per step) exceed the 126 MB L2; no flush needed",
-                   "parallelism": f"streams x{world} (one independent stream per GPU)"},
-        "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
-                     "traffic": traffic, "kernel": "dedisperse (K3)",
-                     "convention": "no-reuse effective bytes NCHANOUT*4 per DM-trial.sample (values > 1 = on-chip "
-                                   "reuse); peak " + peak_src,
-                     "compulsory_gbs": comp_bytes / (k3_ms / 1000.0) / 1e9,
-                     "add_rate_tadd_s": adds_per_s / 1e12,
-                     "fp32_add_peak_frac": adds_per_s / fp32_peak_adds},
+        "config": bench_config(data_s, world),
+        "roofline": roofline,
         "clocks": f32["clocks"],
         "stages_ms_per_step": {"channelise_K1": f32["stage_ms"][0], "bandpass_K2": f32["stage_ms"][1],
                                "dedisperse_stats_K3": f32["stage_ms"][2]},
@@ -636,7 +742,7 @@ def main():
                                    "h2d_bytes_per_step": int(e2e16["h2d"]), "d2h_bytes_per_step": int(e2e16["d2h"])}
     if not args.skip_extras:
         try:
-            line["cpu_baseline"] = {k: v for k, v in cpu_baseline(args.cpu_sample).items() if k != "seconds"}
+            line["cpu_baseline"] = {k: v for k, v in cpu_baseline(args.cpu_sample, min_cpu_s=10.0).items() if k != "seconds"}
         except Exception as e:  # noqa: BLE001
             line["cpu_baseline"] = {"value": None, "error": str(e)[:200]}
         try:
@@ -658,11 +764,27 @@ def main():
             dsnr = max((abs(x[3] - y[3]) / x[3] for x, y in zip(cl["fp32"], cl["fp16"])), default=0.0) if same \
                 else None
             line["serving"] = {"streams": 16, "arrivals": "Poisson, 1.5x real time (after a back-to-back fill past "
-                                                          "the 12.4-s overlap)",
-                               "chunk_bytes": "U(0.5, 2.0) s, not frame-aligned", "output_chunk_ms": 1000.0,
-                               **sv, "candidates_identical": same, "max_dsnr": dsnr}
+                                                          "every pulse's chunk and the 12.4-s overlap)",
+                               "chunk_bytes": "U(0.5, 8.0) s, not frame-aligned", "output_chunk_ms": 1000.0,
+                               "input": "page-locked host memory", **sv, "candidates_identical": same,
+                               "max_dsnr": dsnr}
         except Exception as e:  # noqa: BLE001
             line["serving"] = {"error": str(e)[:200]}
+        try:
+            cap = {}
+            for name, st in (("fp32", 0), ("fp16", 1)):
+                r = run_capacity(vf, st)
+                lt = r["lat"]
+                cap[name] = {"rtf": r["rtf"], "p50_ms": float(np.percentile(lt, 50)),
+                             "p99_ms": float(np.percentile(lt, 99)), "results": int(lt.size),
+                             "data_seconds": r["data_s"], "wall_s": r["wall"]}
+            line["capacity"] = {"streams": 16, "chunk_bytes": "U(0.5, 8.0) s, not frame-aligned, random stream order, "
+                                                              "as fast as accepted",
+                                "input": "device memory (vfrb_push_frames from the GPU: no PCIe)",
+                                "output_chunk_ms": 1000.0, **cap,
+                                "fp16_over_fp32": cap["fp16"]["rtf"] / cap["fp32"]["rtf"]}
+        except Exception as e:  # noqa: BLE001
+            line["capacity"] = {"error": str(e)[:200]}
     line["e2e_candidates"] = len(e2e["cands"])
     # the same candidates clustered across trials and chunks (vfrb_cluster_cands:
     # within 16 trials and 50 samples), i.e. one entry per detected pulse

@@ -227,7 +227,11 @@ int vfrb_dedisperse(const vfrb_ddplan* plan, const vfrb_dd_args* a, void* stream
  * ignored; this call allocates nothing.  Requests whose
  * vfrb_dedisperse_workspace_bytes exceed that size return VFRB_ERR_ARG and
  * launch nothing.  The first call on each device looks up the array's
- * address (make it before any stream capture).  All calls on one device
+ * address (make it before any stream capture); the address is looked up
+ * again when the device's current CUDA context changes (another context
+ * made current, the primary context re-created after cudaDeviceReset), and
+ * the first call after such a change should likewise come before any
+ * stream capture.  All calls on one device
  * share the array: calls whose work overlaps on the GPU (other streams,
  * other threads) race and corrupt each other's statistics, so order them
  * on one stream.  Nothing in the array needs to start at zero. */
@@ -298,7 +302,9 @@ int vfrb_fb_to_time_major(const float* src_cm, int64_t chan_stride, int64_t row0
 #define VFRB_OUT_DEDISP 1          /* dedispersed series [ndm][nt]          */
 #define VFRB_OUT_DMSTATS 2         /* per-DM ave/sigma/peak/FRB/argmax      */
 #define VFRB_OUT_SIGMA 4           /* per-sample channel sigma (TS)         */
-#define VFRB_OUT_CHANSTATS 8       /* per-channel statistics (STATS)        */
+#define VFRB_OUT_CHANSTATS 8       /* per-channel statistics (STATS); stream
+                                      mode: FP32 form, one result per absolute
+                                      TIMESTATS block (see vfrb_result)     */
 #define VFRB_OUT_FB 16             /* bandpass-subtracted FB, time-major    */
 #define VFRB_OUT_CANDS 32          /* candidate list                        */
 #define VFRB_OUT_FLAGS 64          /* per-row data flags (VFRB_ROW_*)       */
@@ -388,7 +394,11 @@ typedef struct vfrb_result {
   int32_t nchan;
   int64_t fb_rows;
   const float* fb;                 /* [fb_rows][nchan] or NULL               */
-  int32_t nstatblks;
+  int32_t nstatblks;               /* block mode: TIMESTATS blocks of the
+                                    * block; stream mode: 1 in the result of
+                                    * one statistics block (rows [row0, row0 +
+                                    * nflag_rows or TIMESTATS rows), nt = 0),
+                                    * 0 in series results                  */
   const float* chan_ave;           /* [nstatblks][nchan] each, or NULL       */
   const float* chan_sig;
   const float* chan_outlier;
@@ -415,8 +425,11 @@ int64_t vfrb_plan_device_bytes(const vfrb_plan* plan);
 
 /* Feed raw VDIF bytes of one stream (any split; frames may straddle calls).
  * nbytes == 0 marks end of data (the reference's EOF/EOD).  Page-locked
- * input is copied to the device directly, other input through a staging
- * buffer; `bytes` may be reused as soon as the call returns. */
+ * input is copied to the device directly, other host input through a
+ * staging buffer; `bytes` may also be device memory of the plan's device
+ * (frames already on the GPU, e.g. from a capture kernel): they are copied
+ * device to device and only their 32-byte headers go to the host for the
+ * pair reader.  `bytes` may be reused as soon as the call returns. */
 int vfrb_push_frames(vfrb_plan* plan, int stream, const uint8_t* bytes, size_t nbytes);
 
 /* Streams opened and closed while others run (serving).  vfrb_stream_open

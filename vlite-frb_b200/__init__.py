@@ -470,7 +470,9 @@ class Plan:
         return True
 
     def push(self, stream: int, data):
-        """data: bytes / numpy uint8 / torch uint8 CPU tensor (pinned or not); None = end of data."""
+        """data: bytes / numpy uint8 / torch uint8 tensor -- CPU (pinned or not)
+        or CUDA (device-resident frames are copied on the device, only their
+        headers go to the host); None = end of data."""
         if data is None:
             _check(_lib.vfrb_push_frames(self._h, stream, None, 0), "vfrb_push_frames")
             return

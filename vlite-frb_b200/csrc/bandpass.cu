@@ -208,9 +208,9 @@ int launch_chan_stats(const vfrb_cs_args& a, cudaStream_t s) {
 // (steady tones) or far above it (bursts); a one-row block gives inf/NaN as
 // M - 1 = 0.  FP64 sums.  The FB is time-major,
 // so a warp reads 32 consecutive channels of a row: 128-byte segments.
-__global__ void __launch_bounds__(256) k_chan_sk(const float* __restrict__ fb, long long row_stride, int nchan,
-                                                 int nrows, int ncolstatblk, int nstatblks, double nsum,
-                                                 float* __restrict__ sk) {
+__global__ void __launch_bounds__(256) k_chan_sk(const float* __restrict__ fb, long long row_stride, long long row0,
+                                                 unsigned long long row_mask, int nchan, int nrows, int ncolstatblk,
+                                                 int nstatblks, double nsum, float* __restrict__ sk) {
   const int c = blockIdx.x * 256 + threadIdx.x;
   const int k = blockIdx.y;
   if (c >= nchan || k >= nstatblks) return;
@@ -218,7 +218,7 @@ __global__ void __launch_bounds__(256) k_chan_sk(const float* __restrict__ fb, l
   const long long r1 = min(r0 + ncolstatblk, (long long)nrows);
   double s1 = 0.0, s2 = 0.0;
   for (long long r = r0; r < r1; ++r) {
-    const double x = (double)fb[r * row_stride + c];
+    const double x = (double)fb[(long long)((unsigned long long)(row0 + r) & row_mask) * row_stride + c];
     s1 += x;
     s2 += x * x;
   }
@@ -227,14 +227,22 @@ __global__ void __launch_bounds__(256) k_chan_sk(const float* __restrict__ fb, l
   sk[(long long)k * nchan + c] = (float)v;
 }
 
-int launch_chan_sk(const float* fb_tm, long long row_stride, int nchan, int nrows, int ncolstatblk, int nstatblks,
-                   int nsum, float* sk, cudaStream_t s) {
+// rows r < nrows of the block start at ring row (row0 + r) & row_mask
+// (row_mask ~0: a linear array)
+int launch_chan_sk_ring(const float* fb_tm, long long row_stride, long long row0, unsigned long long row_mask,
+                        int nchan, int nrows, int ncolstatblk, int nstatblks, int nsum, float* sk, cudaStream_t s) {
   if (!fb_tm || !sk || nchan <= 0 || nstatblks <= 0 || ncolstatblk <= 1 || nsum < 1 || row_stride < nchan ||
-      (long long)nrows - (long long)ncolstatblk * (nstatblks - 1) < 1 || nstatblks > 65535)
+      (long long)nrows - (long long)ncolstatblk * (nstatblks - 1) < 1 || nstatblks > 65535 || row0 < 0)
     return VFRB_ERR_ARG;
   dim3 grid((unsigned)((nchan + 255) / 256), (unsigned)nstatblks);
-  k_chan_sk<<<grid, 256, 0, s>>>(fb_tm, row_stride, nchan, nrows, ncolstatblk, nstatblks, (double)nsum, sk);
+  k_chan_sk<<<grid, 256, 0, s>>>(fb_tm, row_stride, row0, row_mask, nchan, nrows, ncolstatblk, nstatblks,
+                                 (double)nsum, sk);
   return cuda_status(cudaGetLastError());
+}
+
+int launch_chan_sk(const float* fb_tm, long long row_stride, int nchan, int nrows, int ncolstatblk, int nstatblks,
+                   int nsum, float* sk, cudaStream_t s) {
+  return launch_chan_sk_ring(fb_tm, row_stride, 0, ~0ULL, nchan, nrows, ncolstatblk, nstatblks, nsum, sk, s);
 }
 
 // ---- channel-major -> time-major copy ---------------------------------------

@@ -713,7 +713,6 @@ int launch_dedisperse_plan(const vfrb_ddplan* pl, const vfrb_dd_args& a, cudaStr
     return VFRB_ERR_ARG;
   int v = pl->variant[a.storage];
   if (v == VFRB_DD_AUTO) v = default_variant(pl, a.storage);
-  if (getenv("VFRB_DD_V1")) v = VFRB_DD_STAGED;
   return launch_variant(pl, v, a, s);
 }
 

@@ -165,6 +165,7 @@ struct StreamSt {
   Owned res;
   cudaStream_t cs = nullptr;   // compute
   cudaStream_t xs = nullptr;   // host-to-device copies
+  cudaStream_t hs = nullptr;   // header copies of device-resident input
   cudaEvent_t ev_copied = nullptr, ev_consumed = nullptr;
   // Release events: one per channeliser launch, with the oldest frame any
   // later work still reads (frames below it are free once the event has
@@ -212,6 +213,7 @@ struct StreamSt {
   int64_t R1 = 0;
   int64_t rows_chan = 0, rows_bp = 0, rows_out = 0;
   int64_t chunks = 0;
+  int64_t stat_blocks = 0;     // TIMESTATS blocks emitted (VFRB_OUT_CHANSTATS)
   // both
   void* d_cm = nullptr;  // channel-major bandpassed FB (storage form)
   int64_t cm_stride = 0;
@@ -257,13 +259,19 @@ struct vfrb_plan {
 
 namespace {
 
-bool is_pinned(const void* p) {
+// Where pushed bytes live: pageable host memory (copied through staging
+// buffers), page-locked host memory (copied to the device in place), or
+// device memory (copied device to device; only headers go to the host).
+enum MemKind { kPageable = 0, kPinned = 1, kDevice = 2 };
+MemKind mem_kind(const void* p) {
   cudaPointerAttributes a{};
   if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
     cudaGetLastError();
-    return false;
+    return kPageable;
   }
-  return a.type == cudaMemoryTypeHost;
+  if (a.type == cudaMemoryTypeHost) return kPinned;
+  if (a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged) return kDevice;
+  return kPageable;
 }
 
 template <typename T>
@@ -321,6 +329,7 @@ int64_t stream_bytes(const vfrb_plan* pl, int64_t ring_frames, int64_t R1, int64
     if (want(pl, VFRB_OUT_CHANSTATS)) b += 3LL * pl->nstatblks * nch * 4;
   } else {
     b += R1 * nch * 4 + R2 * nch * (int64_t)storage_bytes(P.storage);
+    if (want(pl, VFRB_OUT_CHANSTATS)) b += 4LL * nch * 4;
   }
   if (pl->want_dd) {
     b += (int64_t)pl->ndm * nt * 4 * (want(pl, VFRB_OUT_SIGMA) ? 2 : 1);
@@ -359,7 +368,7 @@ int alloc_slot(vfrb_plan* pl, StreamSt* s, ResultSlot** out) {
     }
   }
   if (P.mode == VFRB_MODE_BLOCK && want(pl, VFRB_OUT_FB)) ST(hmalloc(s->res, &r->fb, (size_t)pl->L.maxnt * nch * 4));
-  if (P.mode == VFRB_MODE_BLOCK && want(pl, VFRB_OUT_CHANSTATS)) {
+  if (want(pl, VFRB_OUT_CHANSTATS)) {
     ST(hmalloc(s->res, &r->cave, (size_t)pl->nstatblks * nch * 4));
     ST(hmalloc(s->res, &r->csig, (size_t)pl->nstatblks * nch * 4));
     ST(hmalloc(s->res, &r->cout, (size_t)pl->nstatblks * nch * 4));
@@ -722,6 +731,68 @@ int chunk_stats(vfrb_plan* pl, StreamSt* s, int64_t col0, int64_t nt) {
   return VFRB_OK;
 }
 
+// Stream mode, VFRB_OUT_CHANSTATS: statistics of TIMESTATS block k (rows
+// [k*ncol, (k+1)*ncol) of the stream), once the bandpass has covered it, as
+// a result of its own (nstatblks = 1, no series): calcstats per channel
+// (STATS:910-946) of the bandpassed FP32 rows in the channel-major ring, and
+// the spectral kurtosis of the raw rows still in the raw ring.
+int stream_stats_block(vfrb_plan* pl, StreamSt* s, int64_t k) {
+  const Range nvtx_range("vfrb stream stats");
+  const vfrb_layout& L = pl->L;
+  const int64_t nch = L.nchanout;
+  const int64_t row0 = k * pl->ncolstatblk;
+  vfrb_cs_args c{};
+  c.fb = (const float*)s->d_cm;
+  c.chan_stride = s->cm_stride;
+  c.row0 = row0;
+  c.row_mask = s->cm_mask;
+  c.nchan = (int32_t)nch;
+  c.nrows = pl->ncolstatblk;
+  c.ncolstatblk = pl->ncolstatblk;
+  c.nstatblks = 1;
+  c.ave = s->d_cave;
+  c.sig = s->d_csig;
+  c.outlier = s->d_cout;
+  ST(launch_chan_stats(c, s->cs));
+  ST(launch_chan_sk_ring(s->d_raw, nch, row0, (unsigned long long)(s->R1 - 1), (int)nch, pl->ncolstatblk,
+                         pl->ncolstatblk, 1, 2 * L.nave, s->d_csk, s->cs));
+  ResultSlot* r = nullptr;
+  ST(alloc_slot(pl, s, &r));
+  const size_t b = (size_t)nch * 4;
+  CK(cudaMemcpyAsync(r->cave, s->d_cave, b, cudaMemcpyDeviceToHost, s->cs));
+  CK(cudaMemcpyAsync(r->csig, s->d_csig, b, cudaMemcpyDeviceToHost, s->cs));
+  CK(cudaMemcpyAsync(r->cout, s->d_cout, b, cudaMemcpyDeviceToHost, s->cs));
+  CK(cudaMemcpyAsync(r->csk, s->d_csk, b, cudaMemcpyDeviceToHost, s->cs));
+  r->flags.clear();
+  if (want(pl, VFRB_OUT_FLAGS)) {
+    r->flags.resize((size_t)pl->ncolstatblk);
+    for (int64_t i = 0; i < pl->ncolstatblk; ++i) r->flags[(size_t)i] = s->rflags[(size_t)((row0 + i) & s->fmask)];
+  }
+  CK(cudaMemcpyAsync(r->err, s->d_err, 4, cudaMemcpyDeviceToHost, s->cs));
+  CK(cudaMemsetAsync(s->d_err, 0, 4, s->cs));
+  r->t_done = 0.0;
+  CK(cudaLaunchHostFunc(s->cs, mark_done, r));
+  CK(cudaEventRecord(r->ev, s->cs));
+  vfrb_result& o = r->r;
+  o = vfrb_result{};
+  o.stream = s->id;
+  o.seq = k;
+  o.row0 = row0;
+  o.tstart_mjd = s->tstart_mjd;
+  o.nchan = (int32_t)nch;
+  o.nstatblks = 1;
+  o.chan_ave = r->cave;
+  o.chan_sig = r->csig;
+  o.chan_outlier = r->cout;
+  o.chan_sk = r->csk;
+  o.nflag_rows = (int64_t)r->flags.size();
+  o.row_flags = r->flags.empty() ? nullptr : r->flags.data();
+  r->t_data = s->t_push;
+  r->state = 1;
+  pl->queue.push_back(r);
+  return VFRB_OK;
+}
+
 // k output chunks of nt samples each with one dedispersion launch
 int stream_chunks(vfrb_plan* pl, StreamSt* s, int64_t k, int64_t nt) {
   const Range nvtx_range("vfrb stream chunks");
@@ -763,10 +834,13 @@ int process(vfrb_plan* pl, StreamSt* s, bool final_flush) {
     }
     return VFRB_OK;
   }
+  const bool stats = want(pl, VFRB_OUT_CHANSTATS);
   for (;;) {
     const int64_t avail = npairs(s) * kDataLen / S;
     int64_t n = std::min(avail - s->rows_chan, pl->launch_rows);
     n = std::min(n, s->R1 - 256 - (s->rows_chan - s->rows_bp));
+    // the raw rows of the statistics block in progress stay in the raw ring
+    if (stats) n = std::min(n, s->R1 - (s->rows_chan - s->stat_blocks * pl->ncolstatblk));
     if (n <= 0) break;
     ST(launch_rows(pl, s, s->rows_chan, n, s->d_raw, s->rows_chan, (unsigned)(s->R1 - 1)));
     s->rows_chan += n;
@@ -775,6 +849,10 @@ int process(vfrb_plan* pl, StreamSt* s, bool final_flush) {
     if (w1 > s->rows_bp) {
       ST(run_bandpass(pl, s, s->d_raw, s->rows_bp, (unsigned)(s->R1 - 1), w1 - s->rows_bp, s->rows_bp, nullptr));
       s->rows_bp = w1;
+    }
+    while (stats && (s->stat_blocks + 1) * pl->ncolstatblk <= s->rows_bp) {
+      ST(stream_stats_block(pl, s, s->stat_blocks));
+      ++s->stat_blocks;
     }
     if (pl->want_dd)
       for (;;) {  // a backlog of chunks is dedispersed in one launch (fills the GPU better)
@@ -819,15 +897,17 @@ int64_t oldest_ref(const StreamSt* s) {
 }
 
 // Copy `nf` whole frames to the ring, queue their headers, advance.
-int feed_frames(vfrb_plan* pl, StreamSt* s, const uint8_t* host, int64_t nf, bool pinned) {
+int feed_frames(vfrb_plan* pl, StreamSt* s, const uint8_t* in, int64_t nf, MemKind kind) {
   const Range nvtx_range("vfrb feed frames");
+  const bool pinned = kind == kPinned, device = kind == kDevice;
   // page-locked input is copied in place, in quarters of the ring; other
-  // input goes through the (smaller) staging buffers
+  // input goes through the (smaller) staging buffers, whose frame count also
+  // bounds a batch of device input (its headers are brought there)
   const int64_t batch_max =
       std::max<int64_t>(1, pinned ? s->ring_frames / 4 : std::min<int64_t>(s->ring_frames / 4, (int64_t)s->stage_frames));
   for (int64_t done = 0; done < nf;) {
     const int64_t nb = std::min(batch_max, nf - done);
-    const uint8_t* src = host + done * kFrameLen;
+    const uint8_t* src = in + done * kFrameLen;  // host bytes, or device bytes (device input)
     // frames about to be overwritten must have been consumed by launched work
     if (oldest_ref(s) < s->frames_in + nb - s->ring_frames) {
       ST(process(pl, s, false));
@@ -850,7 +930,24 @@ int feed_frames(vfrb_plan* pl, StreamSt* s, const uint8_t* host, int64_t nf, boo
       CK(cudaStreamWaitEvent(s->xs, wait_ev, 0));
     }
     const uint8_t* from = src;
-    if (!pinned) {
+    if (device) {
+      // headers to the host (32 bytes a frame, into a staging buffer with the
+      // frame pitch, where the reader reads them), frames device to device
+      const int k = s->stage_i;
+      s->stage_i = (s->stage_i + 1) % kStageBufs;
+      CK(cudaEventSynchronize(s->stage_ev[k]));
+      CK(cudaMemcpy2DAsync(s->h_stage[k], kFrameLen, src, kFrameLen, kHdrLen, (size_t)nb, cudaMemcpyDeviceToHost,
+                           s->hs));
+      const int64_t slot0 = s->frames_in % s->ring_frames;
+      const int64_t n1 = std::min(nb, s->ring_frames - slot0);
+      CK(cudaMemcpyAsync(s->d_frames + slot0 * kFrameLen, src, (size_t)n1 * kFrameLen, cudaMemcpyDeviceToDevice, s->xs));
+      if (nb > n1)
+        CK(cudaMemcpyAsync(s->d_frames, src + n1 * kFrameLen, (size_t)(nb - n1) * kFrameLen, cudaMemcpyDeviceToDevice,
+                           s->xs));
+      CK(cudaStreamSynchronize(s->hs));
+      CK(cudaEventRecord(s->stage_ev[k], s->hs));
+      src = s->h_stage[k];  // the reader and the flags below read the headers only
+    } else if (!pinned) {
       const int k = s->stage_i;
       s->stage_i = (s->stage_i + 1) % kStageBufs;
       CK(cudaEventSynchronize(s->stage_ev[k]));
@@ -890,7 +987,7 @@ int feed_frames(vfrb_plan* pl, StreamSt* s, const uint8_t* host, int64_t nf, boo
     ST(process(pl, s, false));
     done += nb;
   }
-  if (pinned) CK(cudaEventSynchronize(s->ev_copied));  // the caller may reuse its buffer on return
+  if (pinned || device) CK(cudaEventSynchronize(s->ev_copied));  // the caller may reuse its buffer on return
   return VFRB_OK;
 }
 
@@ -916,6 +1013,7 @@ int create_stream(vfrb_plan* pl, int id, int64_t ring_frames, int64_t R1, int64_
                                            P.dada_skip != 0);
   ST(mkstream(s->res, &s->cs));
   ST(mkstream(s->res, &s->xs));
+  ST(mkstream(s->res, &s->hs));
   ST(mkevent(s->res, &s->ev_copied));
   ST(mkevent(s->res, &s->ev_consumed));
   for (auto& e : s->rel_ev) ST(mkevent(s->res, &e));
@@ -969,6 +1067,12 @@ int create_stream(vfrb_plan* pl, int id, int64_t ring_frames, int64_t R1, int64_
     s->cm_mask = (unsigned)(R2 - 1);
     ST(dmalloc(s->res, &s->d_cm, (size_t)nch * R2 * sb));
     CK(cudaMemsetAsync(s->d_cm, 0, (size_t)nch * R2 * sb, s->cs));
+    if (want(pl, VFRB_OUT_CHANSTATS)) {
+      ST(dmalloc(s->res, &s->d_cave, (size_t)nch * 4));
+      ST(dmalloc(s->res, &s->d_csig, (size_t)nch * 4));
+      ST(dmalloc(s->res, &s->d_cout, (size_t)nch * 4));
+      ST(dmalloc(s->res, &s->d_csk, (size_t)nch * 4));
+    }
     nt = pl->chunk_rows * pl->batch_chunks;
     // rows from the oldest not yet emitted to the newest channelised: at
     // most R2 (channel-major ring) + R1 (raw ring)
@@ -1094,6 +1198,13 @@ int vfrb_plan_create(vfrb_plan** out, const vfrb_params* prm) {
     }
   } else {
     pl->chunk_rows = std::max<int64_t>(32, (int64_t)llround(P.chunk_seconds / L.tchan));
+    if (P.outputs & VFRB_OUT_CHANSTATS) {
+      // absolute TIMESTATS blocks of the stream, one result each
+      pl->nstatblks = 1;
+      pl->ncolstatblk = (int)((double)P.timestats / L.tchan);  // STATS:211
+      if (pl->ncolstatblk < 2) return fail(VFRB_ERR_ARG);
+      if (P.storage != VFRB_F32) return fail(VFRB_ERR_UNSUPPORTED);
+    }
   }
   const int64_t S = (int64_t)L.nave * L.twonchan;
   int64_t ring_frames = std::max<int64_t>(4 * (2 * kFramesPerCal + 16), (int64_t)(P.ring_seconds * kFramesPerSec * 2));
@@ -1110,9 +1221,12 @@ int vfrb_plan_create(vfrb_plan** out, const vfrb_params* prm) {
     // a backlog of chunks is dedispersed in launches of about 4096 samples
     pl->batch_chunks = std::min<int64_t>(8, std::max<int64_t>(1, (4096 + pl->chunk_rows - 1) / pl->chunk_rows));
   }
-  const int64_t R1 = (int64_t)pow2_at_least((unsigned long long)(pl->launch_rows + 512));
-  const int64_t R2 = (int64_t)pow2_at_least(
-      (unsigned long long)(pl->max_delay + pl->chunk_rows * pl->batch_chunks + pl->launch_rows + 512));
+  // stream mode with statistics: both rings also hold a statistics block
+  // and the rows channelised past it
+  const int64_t stat_rows = (P.mode == VFRB_MODE_STREAM && pl->ncolstatblk > 0) ? pl->ncolstatblk + pl->launch_rows : 0;
+  const int64_t R1 = (int64_t)pow2_at_least((unsigned long long)std::max(pl->launch_rows + 512, stat_rows + 512));
+  const int64_t R2 = (int64_t)pow2_at_least((unsigned long long)std::max(
+      pl->max_delay + pl->chunk_rows * pl->batch_chunks + pl->launch_rows + 512, stat_rows + 512));
   pl->ring_frames = ring_frames;
   pl->R1 = R1;
   pl->R2 = R2;
@@ -1216,21 +1330,36 @@ int vfrb_push_frames(vfrb_plan* pl, int stream, const uint8_t* bytes, size_t nby
     s->ended = true;
     return s->reader_error;
   }
-  const bool pinned = is_pinned(bytes);
+  const MemKind kind = mem_kind(bytes);
+  // bytes of a frame split across calls are assembled on the host (device
+  // input: the few bytes of the head and tail are copied down first)
+  auto host_bytes = [&](size_t off, size_t n, std::vector<uint8_t>& dst) -> int {
+    const size_t at = dst.size();
+    dst.resize(at + n);
+    if (kind == kDevice) {
+      CK(cudaMemcpy(dst.data() + at, bytes + off, n, cudaMemcpyDeviceToHost));
+    } else {
+      std::memcpy(dst.data() + at, bytes + off, n);
+    }
+    return VFRB_OK;
+  };
   size_t pos = 0;
   if (!s->part.empty()) {
     const size_t take = std::min(nbytes, (size_t)kFrameLen - s->part.size());
-    s->part.insert(s->part.end(), bytes, bytes + take);
+    ST(host_bytes(0, take, s->part));
     pos = take;
     if (s->part.size() == (size_t)kFrameLen) {
-      ST(feed_frames(pl, s, s->part.data(), 1, false));
+      ST(feed_frames(pl, s, s->part.data(), 1, kPageable));
       s->part.clear();
     }
   }
   const int64_t whole = (int64_t)((nbytes - pos) / kFrameLen);
-  if (whole > 0) ST(feed_frames(pl, s, bytes + pos, whole, pinned));
+  if (whole > 0) ST(feed_frames(pl, s, bytes + pos, whole, kind));
   pos += (size_t)whole * kFrameLen;
-  if (pos < nbytes) s->part.assign(bytes + pos, bytes + nbytes);
+  if (pos < nbytes) {
+    s->part.clear();
+    ST(host_bytes(pos, nbytes - pos, s->part));
+  }
   return s->reader_error;
 }
 

@@ -30,6 +30,8 @@ int launch_bandpass(const vfrb_bp_args& a, cudaStream_t s);
 int launch_chan_stats(const vfrb_cs_args& a, cudaStream_t s);
 int launch_chan_sk(const float* fb_tm, long long row_stride, int nchan, int nrows, int ncolstatblk, int nstatblks,
                    int nsum, float* sk, cudaStream_t s);
+int launch_chan_sk_ring(const float* fb_tm, long long row_stride, long long row0, unsigned long long row_mask,
+                        int nchan, int nrows, int ncolstatblk, int nstatblks, int nsum, float* sk, cudaStream_t s);
 int launch_fb_transpose(const float* src_cm, long long chan_stride, unsigned row_mask, long long row0,
                         int nchan, int nrows, float* dst_tm, long long dst_row_stride, cudaStream_t s);
 int launch_subtract_bp_full(float* fb, long long chan_stride, long long row0, unsigned row_mask, int nchan,

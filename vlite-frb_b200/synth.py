@@ -46,6 +46,7 @@ class Rfi:
     burst_frac: float = 0.01
     burst_gain: float = 8.0
     invalid_frac: float = 0.10
+    seed: int | None = None       # tones, bursts and flags (None: the stream's seed)
 
 
 @dataclass
@@ -59,6 +60,22 @@ class StreamSpec:
     epoch: int = 30               # 2015-01-01
     nave_for_snr: int = 10
     nchan_for_snr: int = 6250
+    block0: int = 0               # 12500-sample block of the stream where this piece starts (RFI time base)
+
+
+def injected_pulses(seed: int = 1, n: int = 20, duration: float = 60.0, dm_lo: float = 50.0,
+                    dm_hi: float = 1000.0) -> list:
+    """The dispersed pulses of the full-scale workload: n pulses with arrival
+    time U(0.2, duration - 0.5) s at the top of the band, DM U(dm_lo, dm_hi),
+    FWHM U(1, 10) ms and matched-filter SNR U(8, 30), from
+    default_rng(seed + 7).  Returns Pulse objects."""
+    rng = np.random.default_rng(seed + 7)
+    out = []
+    for _ in range(n):
+        dm = float(rng.uniform(dm_lo, dm_hi))
+        out.append(Pulse(float(rng.uniform(0.2, duration - 0.5)), dm, float(rng.uniform(1, 10)),
+                         float(rng.uniform(8, 30))))
+    return out
 
 
 def _headers(nframes_pairs: int, spec: StreamSpec, invalid: np.ndarray | None) -> np.ndarray:
@@ -112,24 +129,43 @@ def _inject(x: torch.Tensor, spec: StreamSpec):
 
 
 def _rfi(x: torch.Tensor, spec: StreamSpec, gen: torch.Generator, pol: int, blk0: int):
+    """x: float32 [nblk, 12500] noise of one pol whose first block is block
+    blk0 of the stream; adds the tones and scales the bursts in place.  The
+    tones A sin(w n + phi) are built per block by angle addition,
+    sin(w (n0 + m) + phi) = sin(w m) cos(w n0 + phi) + cos(w m) sin(w n0 + phi),
+    with the block phases in float64: one float32 matrix product."""
     r = spec.rfi
     dev = x.device
     nblk = x.shape[0]
-    rng = np.random.default_rng(spec.seed * 7919 + 17)
+    rseed = spec.seed if r.seed is None else r.seed
+    rng = np.random.default_rng(rseed * 7919 + 17)
     freqs = rng.uniform(0.0, 64e6, r.n_tones)
     amps = rng.uniform(r.tone_amp[0], r.tone_amp[1], r.n_tones)
     phs = rng.uniform(0, 2 * math.pi, (2, r.n_tones))
-    n = (torch.arange(nblk * NBLK, device=dev, dtype=torch.float64) + blk0 * NBLK) / RATE
     flat = x.view(-1)
     # bursts: 1-ms blocks (128000 samples) with noise scaled by burst_gain
     bl = 128000
-    nb = (flat.numel() + bl - 1) // bl
-    brng = np.random.default_rng(spec.seed * 104729 + 3)
-    hit = np.nonzero(brng.random(nb + blk0 * NBLK // bl + 1)[blk0 * NBLK // bl:][:nb] < r.burst_frac)[0]
+    first = blk0 * NBLK // bl
+    nb = (blk0 * NBLK + flat.numel() + bl - 1) // bl - first
+    brng = np.random.default_rng(rseed * 104729 + 3)
+    hit = np.nonzero(brng.random(first + nb)[first:] < r.burst_frac)[0]
     for b in hit:
-        flat[b * bl:(b + 1) * bl] *= r.burst_gain
-    for i in range(r.n_tones):
-        flat += (amps[i] * torch.sin(2 * math.pi * freqs[i] * n + phs[pol, i])).to(torch.float32)
+        a0 = max(0, (first + b) * bl - blk0 * NBLK)
+        a1 = min(flat.numel(), (first + b + 1) * bl - blk0 * NBLK)
+        if a1 > a0:
+            flat[a0:a1] *= r.burst_gain
+    w = 2 * math.pi * freqs / RATE                                      # rad per sample
+    m = np.arange(NBLK, dtype=np.float64)
+    wm = np.outer(w, m)
+    sc = np.concatenate([amps[:, None] * np.sin(wm), amps[:, None] * np.cos(wm)]).astype(np.float32)
+    th = np.outer((np.arange(nblk, dtype=np.float64) + blk0) * NBLK, w) + phs[pol][None, :]
+    coef = np.concatenate([np.cos(th), np.sin(th)], axis=1).astype(np.float32)  # [nblk, 2*ntones]
+    prev = torch.backends.cuda.matmul.allow_tf32
+    torch.backends.cuda.matmul.allow_tf32 = False
+    try:
+        x += torch.from_numpy(coef).to(dev) @ torch.from_numpy(sc).to(dev)
+    finally:
+        torch.backends.cuda.matmul.allow_tf32 = prev
 
 
 def make_vdif(spec: StreamSpec, device: str | torch.device = "cpu") -> torch.Tensor:
@@ -151,14 +187,14 @@ def make_vdif(spec: StreamSpec, device: str | torch.device = "cpu") -> torch.Ten
                 sub.pulses = [Pulse(p.t0 - b0 * NBLK / RATE, p.dm, p.fwhm_ms, p.snr) for p in spec.pulses]
                 _inject(x, sub)
             if spec.rfi is not None:
-                _rfi(x, spec, gen, pol, b0)
+                _rfi(x, spec, gen, pol, spec.block0 + b0)
             samples[b0 * NBLK:b1 * NBLK] = torch.clamp(torch.round(x + 128.0), 0, 255).to(torch.uint8).view(-1)
         pols.append(samples[:nsamp].view(npairs, DATALEN))
     pay = torch.stack(pols, dim=1)  # [npairs, 2, 5000]
     del pols
     invalid = None
     if spec.rfi is not None and spec.rfi.invalid_frac > 0:
-        irng = np.random.default_rng(spec.seed * 31 + 5)
+        irng = np.random.default_rng(spec.seed * 31 + 5 + spec.frame0)
         invalid = irng.random((npairs, 2)) < spec.rfi.invalid_frac
     hdr = torch.from_numpy(_headers(npairs, spec, invalid)).to(device)
     frames = torch.cat([hdr, pay], dim=2)  # [npairs, 2, 5032]
