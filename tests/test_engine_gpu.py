@@ -400,3 +400,71 @@ def test_stream_boxcar_candidates(vf, O, co):
         for c, w in zip(r["cands"], want):
             assert abs(c["dm_index"] - w[0]) <= 1
             assert abs(c["snr"] - w[3]) <= 0.01 * w[3]
+
+
+def test_stream_mode_chan_stats_sk_and_flags(vf, O, co):
+    """Stream mode with VFRB_OUT_CHANSTATS: one result per absolute TIMESTATS
+    block (rows [k*ncol, (k+1)*ncol)) holding calcstats per channel
+    (STATS:910-946) of the bandpassed rows -- ave and variance within 1e-4 of
+    the FP64 oracle (relative to the channel's level), outlier counts exact --
+    the spectral kurtosis of the raw rows within 1e-3, and the block's row
+    flags identical to the oracle's; RFI-heavy input with gaps.  The same
+    stream among two others, pushed in random splits, gives identical
+    results."""
+    nave, tstat = 2, 0.25
+    buf = _rfi_vdif(2.6, seed=9, drop=(7000, 7001, 40000))
+    others = [_rfi_vdif(1.7, seed=10 + i) for i in range(2)]
+    outputs = vf.OUT_CHANSTATS | vf.OUT_FLAGS
+    _, alone = _stream_run(vf, None, [buf], outputs=outputs, timestats=tstat)
+    _, mixed = _stream_run(vf, None, [others[0], buf, others[1]], outputs=outputs, timestats=tstat,
+                           splits=lambda rng: int(rng.integers(1, 300000)))
+    L = O.Layout(nave=nave, muoslowfreq=384.0, nbundle=1)
+    ncol = int(tstat / L.tchan)
+    rows = _oracle_rows(O, co, buf, L)
+    nbp = rows.shape[0] // 128 * 128
+    bp = co.bandpass(rows[:nbp])
+    flags = O.row_flags(_pair_flags(O, buf, L), L, rows.shape[0])
+    nblk = nbp // ncol
+    res = [r for r in alone[0] if r["nstatblks"] == 1]
+    assert len(res) == nblk >= 3 and [r["row0"] for r in res] == [k * ncol for k in range(nblk)]
+    for k, r in enumerate(res):
+        ave, sig, outl = O.calcstats_chan(bp[k * ncol:(k + 1) * ncol], ncol, 1)
+        scale = np.abs(ave[0]) + np.sqrt(np.abs(sig[0])) + 1e-30
+        assert np.max(np.abs(r["chan_ave"][0] - ave[0]) / scale) <= 1e-4
+        assert np.max(np.abs(r["chan_sig"][0] - sig[0]) / (np.abs(sig[0]) + 1e-30)) <= 1e-4
+        assert np.array_equal(r["chan_outlier"][0], outl[0])
+        sk = O.chan_sk(rows[k * ncol:(k + 1) * ncol], ncol, 1, 2 * nave)
+        e = np.max(np.abs(r["chan_sk"][0] - sk[0]))
+        print(f"stream stats block {k}: SK max abs err {e:.2e}")
+        assert e <= 1e-3
+        assert np.array_equal(r["row_flags"], flags[k * ncol:(k + 1) * ncol])
+    assert any((r["row_flags"] & 2).any() for r in res) and any((r["row_flags"] & 1).any() for r in res)
+    mres = [r for r in mixed[1] if r["nstatblks"] == 1]
+    assert len(mres) == len(res)
+    for a, b in zip(res, mres):
+        for key in ("chan_ave", "chan_sig", "chan_outlier", "chan_sk", "row_flags"):
+            assert np.array_equal(a[key], b[key]), key
+
+
+def test_stream_device_input_matches_host(vf):
+    """Frames pushed from device memory (copied device to device, headers to
+    the host for the reader) give results identical to the same bytes pushed
+    from host memory, with splits that cut frames anywhere."""
+    import torch
+    dms = np.arange(0, 6.0, 0.5, dtype=np.float32)
+    buf = _vdif(1.2, seed=31, pulses=[(0.5, 3.0, 2.0, 30.0)])
+    dev = torch.from_numpy(buf).cuda()
+    cuts = [0, 5031, 77777, 350001, 1000000, 2500003, len(buf)]
+    out = []
+    for src in (buf, dev):
+        plan = vf.Plan(dms, nave=2, muoslowfreq=384.0, mode=vf.MODE_STREAM, chunk_seconds=0.25,
+                       outputs=vf.OUT_DEDISP | vf.OUT_DMSTATS | vf.OUT_FLAGS)
+        for a, b in zip(cuts[:-1], cuts[1:]):
+            plan.push(0, src[a:b])
+        plan.push(0, None)
+        out.append(plan.drain())
+        plan.close()
+    assert len(out[0]) == len(out[1]) > 2
+    for x, y in zip(*out):
+        assert x["row0"] == y["row0"] and np.array_equal(x["dd"], y["dd"])
+        assert np.array_equal(x["row_flags"], y["row_flags"]) and x["device_errors"] == y["device_errors"] == 0

@@ -1,27 +1,35 @@
 // K1: fused channeliser for sm_100a.
 //
-// A persistent CTA (512 threads, one per SM) produces filterbank rows in turn;
-// each row is NAVE consecutive 12500-sample windows of both polarisations.
-// Per window the two real 8-bit streams are packed into one complex sequence
-// z[n] = (x0[n]-128) + i (x1[n]-128) and transformed by a hand-written
-// 12500-point mixed-radix Stockham FFT (radices 25, 25, 20) that lives
-// entirely in shared memory (100 kB).  Because
-//   |X0[k]|^2 + |X1[k]|^2 = (|Z[k]|^2 + |Z[N-k]|^2) / 2,
-// detection, the polarisation sum, /NFREQ, the NAVE average and the NSKIP
-// channel slice are an epilogue on Z.  The -128 offset only changes bin 0,
-// which no output channel uses (NSKIP >= 1), and keeps the FP32 transform
-// well conditioned.  This replaces convertarray, cufftExecR2C, sumpower,
-// avepower and the per-row D2D copies of PIPE:574-632 (STATS:377-405,
-// TS:603-636).
+// Replaces convertarray, cufftExecR2C (x2), sumpower, avepower and the
+// per-row D2D channel-select copies of PIPE:574-632 (STATS:377-405,
+// TS:603-636): raw 8-bit VDIF payload bytes of both polarisations in, one
+// NAVE-averaged, NFREQ-normalised, pol-summed power spectrum row out.
 //
-// Input staging: the raw bytes of the NEXT window (2 x 12500) are copied
-// from the frame ring into a second shared-memory byte buffer with 4-byte
-// cp.async while the current window is transformed, so the global-memory
-// latency is hidden behind the FFT; the byte -> float conversion is fused
-// into the first pass's loads.  Gap frames (slot -1) are zero-filled by the
-// copy itself.
+// The two polarisations' real 12500-sample windows are transformed together:
+// each pol's window becomes a 6250-point complex sequence
+// z[m] = (x[2m] - 128) + i (x[2m+1] - 128), and the two sequences run in
+// lockstep as PolPairs (re = (pol0, pol1), im = (pol0, pol1)), so every
+// butterfly step is one packed FP32 instruction (add/sub/mul/fma .f32x2)
+// for both pols.  The 6250-point Stockham FFT has radices 25, 25, 10 and
+// lives in 100 kB of shared memory.  With Z = FFT(z), H = 6250, N = 12500,
+// W = W_N, the real spectrum of each pol is
+//   X[k] = (A - iC)/2,  X[H-k] = conj(A + iC)/2,
+//   A = Z[k] + conj(Z[H-k]),  B = Z[k] - conj(Z[H-k]),  C = W^k B,
+// so bins k and H-k need only Z[k] and Z[H-k].  The last pass's butterflies
+// j and 625-j hold exactly such pairs (bins j + 625 k and 625-j + 625 (9-k)),
+// so one thread runs both and detects |X0|^2 + |X1|^2 for 20 bins straight
+// from registers; the NAVE average accumulates in the output row itself (the
+// first window of a row stores, later ones add with a reduction nothing waits
+// for), each window pre-scaled by 1/(4 NFREQ NAVE).  The -128 offset only
+// changes bin 0, which no output channel uses (NSKIP >= 1), and keeps the
+// FP32 transform well conditioned.
+//
+// One persistent 256-thread CTA per SM (a radix-25 pol-pair butterfly holds
+// 100 floats, so a thread needs up to 255 registers).  The raw bytes of the
+// next window are copied from the frame ring into a shared-memory byte buffer
+// with 4-byte cp.async while the current window is transformed.
 #include "vfrb_common.cuh"
-#include "dft_codelets.cuh"
+#include "dft_pairs.cuh"
 
 #include <algorithm>
 #include <cmath>
@@ -29,36 +37,32 @@
 
 namespace vfrb {
 
-constexpr int kThreads = 512;
-constexpr int kR1 = 25, kR2 = 25, kR3 = 20;
-constexpr int kM1 = kFftN / kR1;  // 500 butterflies in passes 1 and 2
-constexpr int kM3 = kFftN / kR3;  // 625 butterflies in pass 3
-constexpr int kNs2 = kR1;         // 25
-constexpr int kNs3 = kR1 * kR2;   // 625
+constexpr int kH = kFftN / 2;          // 6250-point complex transform per pol
+constexpr int kPThreads = 256;         // one CTA per SM, 8 warps (up to 255 registers)
+constexpr int kPB = kH / 25;           // 250 butterflies in passes 1 and 2
+constexpr int kPM3 = kH / 10;          // 625 butterflies in pass 3
+constexpr int kPTasks = kPM3 / 2 + 1;  // 313 pass-3 tasks: pairs (j, 625 - j), and j = 0
+constexpr int kStage = 12512;          // one pol's window bytes, padded to 16
 
-// Twiddles, computed on the host in double precision and rounded to float:
-//   g_tw2[r-1][m] = W_625^(m r), m < 25, 1 <= r < 25   (pass 2, Ns = 25)
-//   pass 3 needs W^(j r) = W_12500^(j r) for j < 625, 1 <= r < 20: with
-//   r = 5a + b it is T_a[j] * (W^j)^b, from four tables of 625 entries
-//   (T_0 = W^j, T_1 = W^5j, T_2 = W^10j, T_3 = W^15j) and at most three
-//   multiplications for (W^j)^b -- 20 kB instead of a 95 kB table, four
-//   table loads per butterfly instead of nineteen.
-// Each CTA copies the tables into shared memory once.
-constexpr int kTw2 = (kR2 - 1) * kNs2;  // 600
-constexpr int kTw3 = 4 * kM3;           // 2500
-constexpr int kAccFloats = kFftN / 2 + 2;  // 6252 >= any NCHANOUT
-constexpr int kStage = 12512;              // one pol's window bytes, padded to 16
-__device__ float2 g_tw2[kTw2];
-__device__ float2 g_tw3[kTw3];
-// shared-memory layout (bytes): Z | stage[2 buffers][2 pols] | tw2 | tw3 | acc
-constexpr size_t kSmZ = sizeof(float2) * kFftN;
-constexpr size_t kSmStage = (size_t)4 * kStage;
-constexpr size_t kSmTw2 = sizeof(float2) * kTw2;
-constexpr size_t kSmTw3 = sizeof(float2) * kTw3;
-constexpr size_t kSmem = kSmZ + kSmStage + kSmTw2 + kSmTw3 + sizeof(float) * kAccFloats;
-static_assert(kSmem <= 227 * 1024, "channeliser shared memory");
-static_assert(kSmZ % 16 == 0 && kSmStage % 16 == 0 && kStage % 16 == 0 && kSmTw2 % 16 == 0 && kSmTw3 % 16 == 0,
-              "16-byte aligned regions");
+// Twiddle tables, as (c, c, s, s) so a twiddle is one packed pair per
+// component, computed on the host in double precision:
+//   g_pw2[(r-1)*25 + m] = W_625^(m r)   (pass 2, Ns = 25)
+//   g_pw12[j] = W_12500^j, j < 625       (the real-split twiddle of pass 3;
+//                                         its square W_6250^j seeds pass 3's
+//                                         own twiddles)
+constexpr int kPTw2 = 24 * 25;
+constexpr int kPT12 = 625;
+__device__ float4 g_pw2[kPTw2];
+__device__ float4 g_pw12[kPT12];
+
+// shared memory: Z | tw2 | t12 | codelet constants + W_20 | staged bytes
+// [2 buffers][2 pols][kStage]
+constexpr size_t kPSmZ = sizeof(float4) * kH;
+constexpr size_t kPSmTab = sizeof(float4) * (kPTw2 + kPT12 + kPairTable + 1);
+constexpr size_t kPSmem = kPSmZ + kPSmTab + 4 * kStage;
+static_assert(kPSmem <= 227 * 1024, "channeliser shared memory");
+static_assert(kPB <= kPThreads && kPTasks <= 2 * kPThreads, "pass-3 tasks in two rounds");
+static_assert((kPSmZ + kPSmTab) % 16 == 0 && kStage % 16 == 0, "16-byte aligned staging");
 
 static std::mutex g_tw_mu;
 static bool g_tw_ready[64];
@@ -68,25 +72,18 @@ static int ensure_twiddles() {
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return VFRB_ERR_CUDA;
   std::lock_guard<std::mutex> lk(g_tw_mu);
   if (g_tw_ready[dev]) return VFRB_OK;
-  static float2 h2[kTw2], h3[kTw3];
-  for (int r = 1; r < kR2; ++r)
-    for (int m = 0; m < kNs2; ++m) {
-      const double a = -2.0 * M_PI * (double)((m * r) % 625) / 625.0;
-      h2[(r - 1) * kNs2 + m] = make_float2((float)cos(a), (float)sin(a));
-    }
-  for (int t = 0; t < 4; ++t)
-    for (int m = 0; m < kM3; ++m) {
-      const double a = -2.0 * M_PI * (double)(((long long)(t == 0 ? 1 : 5 * t) * m) % kFftN) / (double)kFftN;
-      h3[t * kM3 + m] = make_float2((float)cos(a), (float)sin(a));
-    }
-  if (cudaMemcpyToSymbol(g_tw2, h2, sizeof(h2)) != cudaSuccess) return VFRB_ERR_CUDA;
-  if (cudaMemcpyToSymbol(g_tw3, h3, sizeof(h3)) != cudaSuccess) return VFRB_ERR_CUDA;
+  static float4 p2[kPTw2], p12[kPT12];
+  auto quad = [](double num, double den) {
+    const double a = -2.0 * M_PI * num / den;
+    return make_float4((float)cos(a), (float)cos(a), (float)sin(a), (float)sin(a));
+  };
+  for (int r = 1; r < 25; ++r)
+    for (int m = 0; m < 25; ++m) p2[(r - 1) * 25 + m] = quad((double)((m * r) % 625), 625.0);
+  for (int j = 0; j < kPT12; ++j) p12[j] = quad((double)j, 12500.0);
+  if (cudaMemcpyToSymbol(g_pw2, p2, sizeof(p2)) != cudaSuccess) return VFRB_ERR_CUDA;
+  if (cudaMemcpyToSymbol(g_pw12, p12, sizeof(p12)) != cudaSuccess) return VFRB_ERR_CUDA;
   g_tw_ready[dev] = true;
   return VFRB_OK;
-}
-
-__device__ __forceinline__ float2 cmul(float2 a, float2 b) {
-  return make_float2(fmaf(a.x, b.x, -a.y * b.y), fmaf(a.x, b.y, a.y * b.x));
 }
 
 __device__ __forceinline__ void cp_async4(void* smem_dst, const void* gsrc, int src_bytes) {
@@ -96,20 +93,56 @@ __device__ __forceinline__ void cp_async4(void* smem_dst, const void* gsrc, int 
 __device__ __forceinline__ void cp_async_commit_k1() { asm volatile("cp.async.commit_group;\n" ::); }
 __device__ __forceinline__ void cp_async_wait_1() { asm volatile("cp.async.wait_group 1;\n" ::); }
 
+// a twiddle c + i s held as packed pairs (both lanes equal); ns = -s
+struct Rot {
+  float2 c, s, ns;
+};
+__device__ __forceinline__ Rot rot_of(float4 q) {
+  return Rot{make_float2(q.x, q.y), make_float2(q.z, q.w), make_float2(-q.z, -q.w)};
+}
+__device__ __forceinline__ Rot rot_mul(const Rot& a, const Rot& b) {
+  return Rot{f2fma(a.s, b.ns, f2mul(a.c, b.c)), f2fma(a.s, b.c, f2mul(a.c, b.s)), f2fma(a.ns, b.c, f2mul(a.c, b.ns))};
+}
+// v *= w, and v *= conj(w)
+__device__ __forceinline__ void pp_mul(PolPair& v, const Rot& w) {
+  const float2 re = f2fma(v.im, w.ns, f2mul(v.re, w.c));
+  v.im = f2fma(v.re, w.s, f2mul(v.im, w.c));
+  v.re = re;
+}
+__device__ __forceinline__ void pp_mulc(PolPair& v, const Rot& w) {
+  const float2 re = f2fma(v.im, w.s, f2mul(v.re, w.c));
+  v.im = f2fma(v.re, w.ns, f2mul(v.im, w.c));
+  v.re = re;
+}
+__device__ __forceinline__ float4 pp_pack(const PolPair& v) { return make_float4(v.re.x, v.re.y, v.im.x, v.im.y); }
+__device__ __forceinline__ PolPair pp_unpack(float4 q) { return PolPair{make_float2(q.x, q.y), make_float2(q.z, q.w)}; }
+
+// A packed point word holds bytes (pol0 sample 2m, pol0 2m+1, pol1 2m,
+// pol1 2m+1).  0x4B0000xx is the float 2^23 + xx; subtracting 2^23 + 128
+// leaves xx - 128 exactly.
+__device__ __forceinline__ PolPair pp_from_word(unsigned w) {
+  const float2 off = f2s(-8388736.0f);
+  const float2 re = make_float2(__uint_as_float(__byte_perm(w, 0x4B000000u, 0x7550)),
+                                __uint_as_float(__byte_perm(w, 0x4B000000u, 0x7552)));
+  const float2 im = make_float2(__uint_as_float(__byte_perm(w, 0x4B000000u, 0x7551)),
+                                __uint_as_float(__byte_perm(w, 0x4B000000u, 0x7553)));
+  return PolPair{f2add(re, off), f2add(im, off)};
+}
+
 // Stage the raw bytes of one 12500-sample window of both pols (stream
-// positions pos0 ..) into st0 / st1.  ALIGNED (sample0 % 4 == 0): 4-byte
-// asynchronous copies, each inside one payload; otherwise synchronous byte
-// loads.  Positions outside the slot table and misaligned payloads set
+// positions pos0 ..) into st0 / st1.  ALIGNED (pos0 % 4 == 0, payloads at
+// 4-byte offsets): 4-byte asynchronous copies, each inside one payload,
+// zero-filled for fill frames (slot -1); otherwise synchronous byte loads.
+// Positions outside the slot table and misaligned payloads set
 // kErrSlotRange and read as zero bytes.
 template <bool ALIGNED>
-__device__ __forceinline__ void stage_window(unsigned char* __restrict__ st0, unsigned char* __restrict__ st1,
-                                             const vfrb_chan_args& a, long long pos0, int& err) {
+__device__ __forceinline__ void pp_stage(unsigned char* __restrict__ st0, unsigned char* __restrict__ st1,
+                                         const vfrb_chan_args& a, long long pos0, int& err) {
   const int tid = threadIdx.x;
   if (ALIGNED) {
-    // one 64-bit division per window; 32-bit arithmetic per 4-byte group
     const long long slot0 = pos0 >= 0 ? pos0 / kDataLen : -1;
     const int off0 = pos0 >= 0 ? (int)(pos0 - slot0 * kDataLen) : 0;
-    for (int g = tid; g < kFftN / 4; g += kThreads) {
+    for (int g = tid; g < kFftN / 4; g += kPThreads) {
       const int o = off0 + 4 * g;  // < 5000 + 12500
       const int q = o / kDataLen;
       const long long slot = slot0 + q;
@@ -129,14 +162,14 @@ __device__ __forceinline__ void stage_window(unsigned char* __restrict__ st0, un
       cp_async4(st1 + 4 * g, s1 >= 0 ? a.frames + s1 + off : a.frames, s1 >= 0 ? 4 : 0);
     }
   } else {
-    for (int n = tid; n < kFftN; n += kThreads) {
+    for (int n = tid; n < kFftN; n += kPThreads) {
       const long long pos = pos0 + n;
-      const long long slot = pos / kDataLen;
-      const int off = (int)(pos - slot * kDataLen);
+      const long long slot = pos >= 0 ? pos / kDataLen : -1;
       unsigned char v0 = 0, v1 = 0;
-      if (pos < 0 || slot >= a.nslots) {
+      if (slot < 0 || slot >= a.nslots) {
         err |= kErrSlotRange;
       } else {
+        const int off = (int)(pos - slot * kDataLen);
         const long long s0 = __ldg(a.slots0 + slot), s1 = __ldg(a.slots1 + slot);
         if (s0 >= 0) v0 = __ldg(a.frames + s0 + off);
         if (s1 >= 0) v1 = __ldg(a.frames + s1 + off);
@@ -147,150 +180,169 @@ __device__ __forceinline__ void stage_window(unsigned char* __restrict__ st0, un
   }
 }
 
-// Passes 1 and 2 of the 12500-point forward FFT of the staged window into Z.
-// Stockham passes: data1[(j/Ns)*Ns*R + j%Ns + r*Ns] = DFT_R(data0[j + r*N/R] * W^(r*(j%Ns)*N/(Ns*R))).
-// Pass 1 reads the staged bytes (not Z), so it needs no barrier between its
-// reads and writes; pass 2 holds its inputs in registers across one barrier,
-// so one Z buffer suffices.
-__device__ __forceinline__ void fft_passes12(float2* __restrict__ Z, const unsigned char* __restrict__ st0,
-                                             const unsigned char* __restrict__ st1, const float2* __restrict__ tw2) {
-  const int tid = threadIdx.x;
-  if (tid < kM1) {  // pass 1: R = 25, Ns = 1 (no twiddles); writes stride 25 (odd -> no bank conflicts)
-    float2 v[kR1];
-#pragma unroll
-    for (int r = 0; r < kR1; ++r)
-      v[r] = make_float2((float)st0[tid + r * kM1] - 128.f, (float)st1[tid + r * kM1] - 128.f);
-    dft25(v);
-#pragma unroll
-    for (int r = 0; r < kR1; ++r) Z[tid * kR1 + r] = v[dft25_pos(r)];
-  }
-  __syncthreads();
-  {  // pass 2: R = 25, Ns = 25
-    float2 v[kR2];
-    const int m = tid % kNs2;
-    if (tid < kM1) {
-#pragma unroll
-      for (int r = 0; r < kR2; ++r) v[r] = Z[tid + r * kM1];
-#pragma unroll
-      for (int r = 1; r < kR2; ++r) v[r] = cmul(v[r], tw2[(r - 1) * kNs2 + m]);
-      dft25(v);
-    }
-    __syncthreads();
-    if (tid < kM1) {
-      const int base = (tid / kNs2) * (kNs2 * kR2) + m;
-#pragma unroll
-      for (int r = 0; r < kR2; ++r) Z[base + r * kNs2] = v[dft25_pos(r)];
-    }
-    __syncthreads();
+// Power of the pol pair into output channel bin - nskip: the first window of
+// a row stores, later ones add (same-thread, same-address order keeps the
+// store first)
+__device__ __forceinline__ void pp_emit(float* dst, int bin, int nskip, int nchanout, bool first, float p) {
+  const int c = bin - nskip;
+  if ((unsigned)c < (unsigned)nchanout) {
+    if (first)
+      dst[c] = p;
+    else
+      atomicAdd(dst + c, p);  // result unused: a reduction, nothing waits for it
   }
 }
 
-// Pass 3 butterfly j (R = 20, Ns = 625): inputs Z[j + 625 r] times W^(j r),
-// output index r in u[dft20_pos(r)] is spectrum bin j + 625 r.
-__device__ __forceinline__ void pass3_butterfly(const float2* __restrict__ Z, const float2* __restrict__ tw3, int j,
-                                                float2 (&u)[kR3]) {
+// Pass 3 (radix 10, Ns = 625) of butterfly j and its mirror 625 - j, the
+// real split and detection.  j = 0 is its own mirror.  kt[kPairTable] holds
+// W_20 = W_12500^625, the step between the bins of one butterfly.
+__device__ __forceinline__ void pp_pass3(const float4* __restrict__ Z, const float4* __restrict__ t12,
+                                         const float4* __restrict__ kt, int j, float* dst, int nskip, int nchanout,
+                                         bool first, float scale) {
+  PolPair u[10], d[10];
+  const Rot q = rot_of(t12[j]);  // W_12500^j
+  if (j == 0) {
 #pragma unroll
-  for (int r = 0; r < kR3; ++r) u[r] = Z[j + r * kM3];
-  const float2 w1 = tw3[j];
-  const float2 w2 = cmul(w1, w1);
-  const float2 w3 = cmul(w2, w1);
-  const float2 w4 = cmul(w3, w1);
-  const float2 t5 = tw3[kM3 + j], t10 = tw3[2 * kM3 + j], t15 = tw3[3 * kM3 + j];
+    for (int r = 0; r < 10; ++r) u[r] = pp_unpack(Z[kPM3 * r]);
+    dft10p(u, kt);
+  } else {
+    const Rot w1 = rot_mul(q, q);  // W_6250^j
+    Rot wr = w1;
+    u[0] = pp_unpack(Z[j]);
+    d[0] = pp_unpack(Z[kPM3 - j]);
 #pragma unroll
-  for (int r = 1; r < kR3; ++r) {
-    const int a = r / 5, b = r % 5;
-    const float2 wb = b == 1 ? w1 : b == 2 ? w2 : b == 3 ? w3 : w4;
-    const float2 ta = a == 1 ? t5 : a == 2 ? t10 : t15;
-    const float2 w = a == 0 ? wb : (b == 0 ? ta : cmul(ta, wb));
-    u[r] = cmul(u[r], w);
+    for (int r = 1; r < 10; ++r) {
+      u[r] = pp_unpack(Z[j + kPM3 * r]);
+      d[r] = pp_unpack(Z[kPM3 - j + kPM3 * r]);
+      // butterfly 625 - j has twiddles W_6250^((625 - j) r) = W_10^r conj(W_6250^(j r));
+      // the W_10^r factor only moves its outputs by one index (below)
+      pp_mul(u[r], wr);
+      pp_mulc(d[r], wr);
+      if (r < 9) wr = rot_mul(wr, w1);
+    }
+    dft10p(u, kt);
+    dft10p(d, kt);
   }
-  dft20(u);
+  Rot wk = q;  // W_12500^(j + 625 k)
+  const int kend = j == 0 ? 6 : 10;
+#pragma unroll
+  for (int k = 0; k < 10; ++k) {
+    if (k < kend) {
+      // Z[k'] with k' = j + 625 k, and Z[H - k'] (butterfly 625 - j, output
+      // 9 - k, which its twiddle shift leaves at index 10 - k)
+      const PolPair zk = u[dft10p_pos(k)];
+      const PolPair zm = j == 0 ? u[dft10p_pos((10 - k) % 10)] : d[dft10p_pos((10 - k) % 10)];
+      const float2 ar = f2add(zk.re, zm.re), ai = f2sub(zk.im, zm.im);
+      const float2 br = f2sub(zk.re, zm.re), bi = f2add(zk.im, zm.im);
+      const float2 cr = f2fma(bi, wk.ns, f2mul(br, wk.c));
+      const float2 ci = f2fma(br, wk.s, f2mul(bi, wk.c));
+      // |A - iC|^2 and |A + iC|^2, summed over the two pols
+      const float2 ur = f2add(ar, ci), ui = f2sub(ai, cr);
+      const float2 vr = f2sub(ar, ci), vi = f2add(ai, cr);
+      const float2 pu = f2fma(ur, ur, f2mul(ui, ui));
+      const float2 pv = f2fma(vr, vr, f2mul(vi, vi));
+      const int bin = j + kPM3 * k;
+      pp_emit(dst, bin, nskip, nchanout, first, (pu.x + pu.y) * scale);
+      if (bin != kH - bin) pp_emit(dst, kH - bin, nskip, nchanout, first, (pv.x + pv.y) * scale);
+      if (k < 9) wk = rot_mul(wk, rot_of(kt[kPairTable]));
+    }
+  }
 }
-
-__device__ __forceinline__ float pw(float2 z) { return fmaf(z.x, z.x, z.y * z.y); }
 
 template <bool ALIGNED>
-__global__ void __launch_bounds__(kThreads, 1) k_channelise(const vfrb_chan_args a) {
+__global__ void __launch_bounds__(kPThreads, 1) k_channelise(const vfrb_chan_args a) {
   extern __shared__ float4 smem_f4[];
-  unsigned char* sm = reinterpret_cast<unsigned char*>(smem_f4);
-  float2* Z = reinterpret_cast<float2*>(sm);
-  unsigned char* stage = sm + kSmZ;  // [2 buffers][2 pols][kStage]
-  float2* tw2 = reinterpret_cast<float2*>(sm + kSmZ + kSmStage);
-  float2* tw3 = reinterpret_cast<float2*>(sm + kSmZ + kSmStage + kSmTw2);
-  // per-bin power accumulators in shared memory; thread j owns the bins of
-  // pass-3 butterflies j and 625 - j in every window
-  float* acc = reinterpret_cast<float*>(sm + kSmZ + kSmStage + kSmTw2 + kSmTw3);
+  float4* Z = smem_f4;
+  float4* tw2 = smem_f4 + kH;
+  float4* t12 = tw2 + kPTw2;
+  float4* ktab = t12 + kPT12;  // codelet constants, then W_20 (pass 3's bin step)
+  unsigned char* stage = reinterpret_cast<unsigned char*>(ktab + kPairTable + 1);  // [2 buffers][2 pols][kStage]
   const int tid = threadIdx.x;
   int err = 0;
-  for (int i = tid; i < kTw2; i += kThreads) tw2[i] = g_tw2[i];
-  for (int i = tid; i < kTw3; i += kThreads) tw3[i] = g_tw3[i];
-  for (int c = tid; c < a.nchanout; c += kThreads) acc[c] = 0.f;
-  const float scale = 1.0f / (2.0f * (float)a.nfreq * (float)a.nave);
-
-  // persistent CTAs: one per SM; this CTA's windows are (row, w) for rows
-  // blockIdx.x + k*gridDim.x, w < NAVE, in that order
-  const long long nrows_cta = (a.nrows - blockIdx.x + gridDim.x - 1) / gridDim.x;
-  const long long nwin = nrows_cta * a.nave;
-  auto win_pos = [&](long long i) {
-    const long long row = blockIdx.x + (i / a.nave) * gridDim.x;
-    return a.sample0 + (row * a.nave + i % a.nave) * (long long)kFftN;
-  };
-  if (nwin > 0) stage_window<ALIGNED>(stage, stage + kStage, a, win_pos(0), err);
+  for (int i = tid; i < kPTw2; i += kPThreads) tw2[i] = g_pw2[i];
+  for (int i = tid; i < kPT12; i += kPThreads) t12[i] = g_pw12[i];
+  if (tid < kPairTable) ktab[tid] = c_pair_table[tid];
+  if (tid == kPairTable)
+    ktab[tid] = make_float4(9.510565163e-01f, 9.510565163e-01f, -3.090169944e-01f, -3.090169944e-01f);
+  // the staging buffers' padding (never written by the copies) holds the
+  // zero read below: 3 ints in each of the 4 pol buffers
+  if (tid < 4 * ((kStage - kFftN) / 4)) {
+    const int b = tid / ((kStage - kFftN) / 4), e = tid % ((kStage - kFftN) / 4);
+    reinterpret_cast<int*>(stage + (size_t)b * kStage + kFftN)[e] = 0;
+  }
+  // NFREQ-normalised pol-summed power, averaged over NAVE (PIPE:1296, 1310);
+  // |X|^2 = |A -+ iC|^2 / 4
+  const float scale = 0.25f / ((float)a.nfreq * (float)a.nave);
+  // persistent CTAs: this CTA's windows are (row, w) for rows
+  // blockIdx.x + k*gridDim.x, w < NAVE, in that order (32-bit bookkeeping:
+  // a launch has fewer than 2^31 rows)
+  const int nrows_cta = (a.nrows - (int)blockIdx.x + (int)gridDim.x - 1) / (int)gridDim.x;
+  const long long win0 = a.sample0 + (long long)blockIdx.x * a.nave * kFftN;  // first window of row blockIdx.x
+  const long long row_step = (long long)gridDim.x * a.nave * kFftN;            // to the CTA's next row
+  if (nrows_cta > 0) pp_stage<ALIGNED>(stage, stage + kStage, a, win0, err);
   cp_async_commit_k1();
-  for (long long i = 0; i < nwin; ++i) {
-    unsigned char* cur = stage + (size_t)(i & 1) * 2 * kStage;
-    unsigned char* nxt = stage + (size_t)((i + 1) & 1) * 2 * kStage;
-    // the buffer of window i+1 was last read by pass 1 of window i-1, which
-    // every thread has left (barriers after passes 1 and 2)
-    if (i + 1 < nwin) stage_window<ALIGNED>(nxt, nxt + kStage, a, win_pos(i + 1), err);
+  int w = 0, rk = 0, buf = 0;  // window within the row, row of this CTA, staging buffer
+#pragma unroll 1
+  while (rk < nrows_cta) {
+    const int row = (int)blockIdx.x + rk * (int)gridDim.x;
+    const int wn = w + 1 < a.nave ? w + 1 : 0, rn = w + 1 < a.nave ? rk : rk + 1;
+    const unsigned char* cur = stage + (size_t)buf * 2 * kStage;
+    unsigned char* nxt = stage + (size_t)(buf ^ 1) * 2 * kStage;
+    // the next window's buffer was last read by pass 1 of the previous
+    // window, which every thread has left (barriers after passes 1 and 2)
+    if (rn < nrows_cta) pp_stage<ALIGNED>(nxt, nxt + kStage, a, win0 + rn * row_step + (long long)wn * kFftN, err);
     cp_async_commit_k1();
-    cp_async_wait_1();  // this thread's copies of window i have landed
-    __syncthreads();    // ... and everybody else's; pass 3 of window i-1 is done with Z
-    fft_passes12(Z, cur, cur + kStage, tw2);
-    // Pass 3 fused with detection.  Bins k = j + 625 r and N - k =
-    // (625 - j) + 625 (19 - r) come from butterflies j and 625 - j, so thread
-    // j computes both and adds |Z_k|^2 + |Z_{N-k}|^2 to the channel of
-    // min(k, N - k) straight from registers (j = 0 pairs with itself):
-    // pass 3 writes nothing back and there is no separate epilogue.
-    if (tid <= kM3 / 2) {
-      const int jj = tid, jp = (kM3 - jj) % kM3;
-      const bool last = (i % a.nave) == a.nave - 1;
-      const long long row = blockIdx.x + (i / a.nave) * gridDim.x;
-      const unsigned long long orow = (unsigned long long)(a.out_row0 + row) & (unsigned long long)a.out_row_mask;
-      float* dst = a.out + (long long)orow * a.out_row_stride;
-      float mag[kR3];
-      float2 u[kR3];
-      if (jj != 0) {
-        pass3_butterfly(Z, tw3, jp, u);
+    cp_async_wait_1();  // this thread's copies of the current window have landed
+    __syncthreads();    // ... and everybody else's; pass 3 of the previous window is done with Z
+    // The tables' addresses, offset by a zero the compiler cannot see through
+    // (the staging padding, read each window): their entries -- constants,
+    // and twiddles fixed per thread -- are then read where used instead of
+    // being kept in registers across the whole loop, which would not fit.
+    const int z = *reinterpret_cast<const volatile int*>(cur + kFftN);
+    const float4* kt = ktab + z;
+    const float4* tw = tw2 + z;
+    const float4* tj = t12 + z;
+    if (tid < kPB) {  // pass 1: R = 25, Ns = 1, from the staged bytes
+      PolPair v[25];
 #pragma unroll
-        for (int r = 0; r < kR3; ++r) mag[r] = pw(u[dft20_pos(r)]);
+      for (int r = 0; r < 25; ++r) {
+        const int o = 2 * (tid + kPB * r);
+        const unsigned w0 = *reinterpret_cast<const unsigned short*>(cur + o);
+        const unsigned w1 = *reinterpret_cast<const unsigned short*>(cur + kStage + o);
+        v[r] = pp_from_word(__byte_perm(w0, w1, 0x5410));
       }
-      pass3_butterfly(Z, tw3, jj, u);
+      dft25p(v, kt);
 #pragma unroll
-      for (int r = 0; r < kR3; ++r) {
-        float p;
-        int bin;
-        if (jj == 0) {  // bins 625 r and 625 (20 - r); r = 10 is the Nyquist bin (counted twice, as N - k = k)
-          if (r == 0 || r > kR3 / 2) continue;
-          p = pw(u[dft20_pos(r)]) + pw(u[dft20_pos(kR3 - r)]);
-          bin = kM3 * r;
-        } else {
-          p = pw(u[dft20_pos(r)]) + mag[kR3 - 1 - r];
-          bin = r < kR3 / 2 ? jj + kM3 * r : jp + kM3 * (kR3 - 1 - r);
-        }
-        const int c = bin - a.nskip;
-        if (c >= 0 && c < a.nchanout) {
-          const float v = acc[c] + p;
-          if (last) {
-            // (|X0|^2 + |X1|^2)/NFREQ averaged over NAVE spectra (PIPE:1296, 1310)
-            dst[c] = v * scale;
-            acc[c] = 0.f;
-          } else {
-            acc[c] = v;
-          }
-        }
+      for (int k = 0; k < 25; ++k) Z[tid * 25 + k] = pp_pack(v[dft25p_pos(k)]);
+    }
+    __syncthreads();
+    {  // pass 2: R = 25, Ns = 25 (inputs held in registers across the barrier)
+      PolPair v[25];
+      const int m = tid % 25;
+      if (tid < kPB) {
+#pragma unroll
+        for (int r = 0; r < 25; ++r) v[r] = pp_unpack(Z[tid + kPB * r]);
+#pragma unroll
+        for (int r = 1; r < 25; ++r) pp_mul(v[r], rot_of(tw[(r - 1) * 25 + m]));
+        dft25p(v, kt);
+      }
+      __syncthreads();
+      if (tid < kPB) {
+        const int base = (tid / 25) * 625 + m;
+#pragma unroll
+        for (int k = 0; k < 25; ++k) Z[base + 25 * k] = pp_pack(v[dft25p_pos(k)]);
       }
     }
+    __syncthreads();
+    const unsigned long long orow = (unsigned long long)(a.out_row0 + row) & (unsigned long long)a.out_row_mask;
+    float* dst = a.out + (long long)orow * a.out_row_stride;
+    // pass 3: butterflies 1..312 and the cheap self-mirror butterfly 0, one
+    // task each (threads 0..56 take a second one)
+    for (int t = tid; t < kPTasks; t += kPThreads)
+      pp_pass3(Z, tj, kt, t + 1 < kPTasks ? t + 1 : 0, dst, a.nskip, a.nchanout, w == 0, scale);
+    w = wn;
+    rk = rn;
+    buf ^= 1;
   }
   if (err && a.d_err) atomicOr(a.d_err, err);
 }
@@ -302,24 +354,22 @@ int launch_channelise(const vfrb_chan_args& a, cudaStream_t s) {
   if (a.nskip < 1 || a.nchanout < 1 || a.nskip + a.nchanout > kFftN / 2 + 1) return VFRB_ERR_ARG;
   int st = ensure_twiddles();
   if (st) return st;
-  const size_t smem = kSmem;
-  const bool aligned = (a.sample0 % 4) == 0;
   int dev = 0, nsm = 148;
   if (cudaGetDevice(&dev) != cudaSuccess ||
       cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || nsm < 1) {
     cudaGetLastError();
     nsm = 148;
   }
+  // persistent: one CTA per SM, rows dealt round robin
   const int grid = (int)std::min<long long>(a.nrows, (long long)nsm);
-  cudaError_t e;
-  if (aligned) {
-    e = cudaFuncSetAttribute(k_channelise<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e == cudaSuccess) k_channelise<true><<<grid, kThreads, smem, s>>>(a);
-  } else {
-    e = cudaFuncSetAttribute(k_channelise<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e == cudaSuccess) k_channelise<false><<<grid, kThreads, smem, s>>>(a);
+  const bool aligned = (a.sample0 % 4) == 0;
+  auto kern = aligned ? k_channelise<true> : k_channelise<false>;
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPSmem);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return VFRB_ERR_CUDA;
   }
-  if (e != cudaSuccess) return VFRB_ERR_CUDA;
+  kern<<<grid, kPThreads, kPSmem, s>>>(a);
   return cuda_status(cudaGetLastError());
 }
 
