@@ -496,6 +496,20 @@ int vfrb_dada_release(vfrb_dada* ring, uint64_t n);
 /* Page-locks this process's mapping of the ring (needs a CUDA device), so
  * vfrb_push_frames copies acquired bytes straight to the device. */
 int vfrb_dada_pin(vfrb_dada* ring);
+/* The header block beside the data block (as a DADA ring's): the writer sets
+ * up to 4096 bytes of text; a reader waits (bounded) for it and copies at
+ * most cap bytes.  Returns the header's length, or -status. */
+int vfrb_dada_set_header(vfrb_dada* ring, const char* text, uint64_t n);
+int64_t vfrb_dada_get_header(vfrb_dada* ring, char* buf, uint64_t cap, int timeout_ms);
+/* Primary read client (ipcio_open 'R', STATS:294, TS:368): the ring's
+ * `iread` names the reader holding the role, -1 = none.  vfrb_dada_open_read
+ * takes it and returns VFRB_ERR while another reader holds it;
+ * vfrb_dada_force_iread clears it (the reference's ipcbuf_force_iread,
+ * STATS:127-134, TS:140-147) and returns the previous holder; closing a
+ * handle gives its role back. */
+int vfrb_dada_iread(const vfrb_dada* ring);
+int vfrb_dada_force_iread(vfrb_dada* ring);
+int vfrb_dada_open_read(vfrb_dada* ring);
 int vfrb_dada_close(vfrb_dada* ring);
 int vfrb_dada_destroy(uint32_t key);
 

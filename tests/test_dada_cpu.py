@@ -31,6 +31,12 @@ def _lib(vf):
     lib.vfrb_dada_acquire.argtypes = [vp, C.POINTER(C.c_void_p), C.c_uint64, C.c_int]
     lib.vfrb_dada_acquire.restype = C.c_int64
     lib.vfrb_dada_release.argtypes = [vp, C.c_uint64]
+    lib.vfrb_dada_set_header.argtypes = [vp, C.c_char_p, C.c_uint64]
+    lib.vfrb_dada_get_header.argtypes = [vp, C.c_char_p, C.c_uint64, C.c_int]
+    lib.vfrb_dada_get_header.restype = C.c_int64
+    lib.vfrb_dada_iread.argtypes = [vp]
+    lib.vfrb_dada_force_iread.argtypes = [vp]
+    lib.vfrb_dada_open_read.argtypes = [vp]
     return lib
 
 
@@ -113,6 +119,9 @@ def test_writer_tool_feeds_reader(vf, tmp_path):
             threading.Event().wait(0.01)
         else:
             pytest.fail("ring never appeared")
+        hdr = C.create_string_buffer(4096)
+        n = lib.vfrb_dada_get_header(r, hdr, 4096, 20000)
+        assert n > 0 and b"ENCODING VDIF" in hdr.raw[:n] and b"x.bin" in hdr.raw[:n]
         got = np.zeros(data.size, np.uint8)
         pos = 0
         while pos < data.size:
@@ -173,6 +182,71 @@ def test_ring_in_place_reading(vf):
         assert np.array_equal(np.concatenate(got), data) and runs > 20
         assert lib.vfrb_dada_release(r, 1) != 0  # nothing left to release
         lib.vfrb_dada_close(r)
+    finally:
+        lib.vfrb_dada_close(w)
+        lib.vfrb_dada_destroy(key)
+
+
+def test_header_block_and_eod_mid_frame(vf):
+    """The header block: a reader's wait for it is bounded (timeout status)
+    until the writer sets it, then the text comes back as written.  End of
+    data in the middle of a frame: the reader gets the whole frames, then a
+    short read with the partial frame, then 0 (ipcio_read at EOD)."""
+    lib = _lib(vf)
+    key = _key()
+    w = C.c_void_p()
+    assert lib.vfrb_dada_create(key, 1 << 16, C.byref(w)) == 0
+    try:
+        r = C.c_void_p()
+        assert lib.vfrb_dada_connect(key, C.byref(r)) == 0
+        buf = C.create_string_buffer(4096)
+        assert lib.vfrb_dada_get_header(r, buf, 4096, 50) == -ERR_TIMEOUT
+        text = b"HDR_VERSION 1.0\nHDR_SIZE 4096\nENCODING VDIF\n"
+        assert lib.vfrb_dada_set_header(w, text, len(text)) == 0
+        assert lib.vfrb_dada_set_header(w, text, 4097) == 4  # larger than the block: VFRB_ERR_ARG
+        n = lib.vfrb_dada_get_header(r, buf, 4096, 50)
+        assert n == len(text) and buf.raw[:n] == text
+        frames = np.random.default_rng(4).integers(0, 256, 2 * 5032 + 2516, dtype=np.uint8)
+        assert lib.vfrb_dada_write(w, frames.ctypes.data, frames.size, 1000) == frames.size
+        assert lib.vfrb_dada_set_eod(w) == 0
+        got = np.zeros(5032, np.uint8)
+        sizes = [lib.vfrb_dada_read(r, got.ctypes.data, 5032, 1000) for _ in range(4)]
+        assert sizes == [5032, 5032, 2516, 0]
+        assert lib.vfrb_dada_eod(r) == 1
+        lib.vfrb_dada_close(r)
+    finally:
+        lib.vfrb_dada_close(w)
+        lib.vfrb_dada_destroy(key)
+
+
+def test_primary_reader_lock_and_iread_force(vf):
+    """One primary read client at a time (ipcio_open 'R'): a second reader's
+    open fails while the first holds the role; forcing iread (the reference
+    tools' ipcbuf_force_iread hack) clears it and returns the holder, after
+    which the second reader opens; the first reader's close then leaves the
+    second's role alone, and the second's close frees it."""
+    lib = _lib(vf)
+    key = _key()
+    w = C.c_void_p()
+    assert lib.vfrb_dada_create(key, 1 << 16, C.byref(w)) == 0
+    try:
+        r1, r2 = C.c_void_p(), C.c_void_p()
+        assert lib.vfrb_dada_connect(key, C.byref(r1)) == 0
+        assert lib.vfrb_dada_connect(key, C.byref(r2)) == 0
+        assert lib.vfrb_dada_iread(r1) == -1
+        assert lib.vfrb_dada_open_read(r1) == 0
+        holder = lib.vfrb_dada_iread(r2)
+        assert holder != -1
+        assert lib.vfrb_dada_open_read(r2) == 2  # VFRB_ERR: another primary reader
+        assert lib.vfrb_dada_force_iread(r2) == holder
+        assert lib.vfrb_dada_iread(r2) == -1
+        assert lib.vfrb_dada_open_read(r2) == 0
+        mine = lib.vfrb_dada_iread(r1)
+        assert mine not in (-1, holder)
+        lib.vfrb_dada_close(r1)
+        assert lib.vfrb_dada_iread(r2) == mine
+        lib.vfrb_dada_close(r2)
+        assert lib.vfrb_dada_iread(w) == -1
     finally:
         lib.vfrb_dada_close(w)
         lib.vfrb_dada_destroy(key)

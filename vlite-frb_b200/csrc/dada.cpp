@@ -11,6 +11,13 @@
 // A reader can also take the bytes in place (acquire / release) from a
 // mapping it page-locked (pin), so that vfrb_push_frames copies them to the
 // device straight from the ring, with no host copy in between.
+//
+// As in a DADA ring, a header block (up to 4096 bytes of text the writer
+// sets) sits beside the data block, and one reader at a time is the primary
+// read client: vfrb_dada_open_read takes the role (ipcio_open 'R') and fails
+// while another reader holds it; the ring's `iread` field names the holder
+// (-1 = none), and vfrb_dada_force_iread clears it the way the reference
+// tools do before opening (ipcbuf_force_iread, STATS:127-134, TS:140-147).
 #include <cuda_runtime.h>
 #include <fcntl.h>
 #include <sys/mman.h>
@@ -36,10 +43,16 @@ struct RingHdr {
   std::atomic<uint64_t> wpos;      // bytes written so far
   std::atomic<uint64_t> rpos;      // bytes consumed so far
   std::atomic<uint32_t> eod;       // writer finished
+  std::atomic<int32_t> iread;      // primary read client's id, -1 = none
+  std::atomic<uint32_t> hdr_len;   // header block length, kNoHeader until set
   uint32_t pad;
 };
 static_assert(sizeof(RingHdr) <= 64, "header fits one cache line");
 constexpr size_t kHdrBytes = 64;
+constexpr size_t kHeaderBlock = 4096;                 // the DADA header block
+constexpr size_t kDataOff = kHdrBytes + kHeaderBlock;  // where the data block starts
+constexpr uint32_t kNoHeader = 0xffffffffu;
+std::atomic<int32_t> g_next_id{1};                    // reader ids of this process
 
 void shm_name(uint32_t key, char* out, size_t n) { std::snprintf(out, n, "/vfrb_dada_%08x", key); }
 
@@ -62,7 +75,15 @@ struct vfrb_dada {
   uint8_t* data = nullptr;
   size_t map_bytes = 0;
   bool pinned = false;
+  int32_t id = 0;        // this handle's reader id (pid-based, never -1)
+  bool primary = false;  // holds the primary read client role
 };
+
+namespace {
+int32_t new_reader_id() {
+  return (int32_t)((((uint32_t)getpid() & 0x7fffu) << 16) | ((uint32_t)g_next_id.fetch_add(1) & 0xffffu));
+}
+}  // namespace
 
 extern "C" {
 
@@ -72,7 +93,7 @@ int vfrb_dada_create(uint32_t key, uint64_t capacity, vfrb_dada** out) {
   shm_name(key, name, sizeof name);
   const int fd = shm_open(name, O_CREAT | O_EXCL | O_RDWR, 0600);
   if (fd < 0) return VFRB_ERR;
-  const size_t bytes = kHdrBytes + capacity;
+  const size_t bytes = kDataOff + capacity;
   if (ftruncate(fd, (off_t)bytes) != 0) {
     close(fd);
     shm_unlink(name);
@@ -91,7 +112,10 @@ int vfrb_dada_create(uint32_t key, uint64_t capacity, vfrb_dada** out) {
   d->h->wpos.store(0);
   d->h->rpos.store(0);
   d->h->eod.store(0);
-  d->data = static_cast<uint8_t*>(p) + kHdrBytes;
+  d->h->iread.store(-1);
+  d->h->hdr_len.store(kNoHeader);
+  d->data = static_cast<uint8_t*>(p) + kDataOff;
+  d->id = new_reader_id();
   d->map_bytes = bytes;
   std::atomic_thread_fence(std::memory_order_release);
   d->h->magic = kMagic;
@@ -106,7 +130,7 @@ int vfrb_dada_connect(uint32_t key, vfrb_dada** out) {
   const int fd = shm_open(name, O_RDWR, 0600);
   if (fd < 0) return VFRB_ERR;
   struct stat sb;
-  if (fstat(fd, &sb) != 0 || (size_t)sb.st_size < kHdrBytes + 4096) {
+  if (fstat(fd, &sb) != 0 || (size_t)sb.st_size < kDataOff + 4096) {
     close(fd);
     return VFRB_ERR;
   }
@@ -114,15 +138,16 @@ int vfrb_dada_connect(uint32_t key, vfrb_dada** out) {
   close(fd);
   if (p == MAP_FAILED) return VFRB_ERR_NOMEM;
   auto* h = static_cast<RingHdr*>(p);
-  if (h->magic != kMagic || kHdrBytes + h->cap != (size_t)sb.st_size) {
+  if (h->magic != kMagic || kDataOff + h->cap != (size_t)sb.st_size) {
     munmap(p, (size_t)sb.st_size);
     return VFRB_ERR;
   }
   auto* d = new vfrb_dada();
   d->key = key;
   d->h = h;
-  d->data = static_cast<uint8_t*>(p) + kHdrBytes;
+  d->data = static_cast<uint8_t*>(p) + kDataOff;
   d->map_bytes = (size_t)sb.st_size;
+  d->id = new_reader_id();
   *out = d;
   return VFRB_OK;
 }
@@ -234,8 +259,47 @@ int vfrb_dada_eod(const vfrb_dada* d) {
          d->h->wpos.load(std::memory_order_acquire) == d->h->rpos.load(std::memory_order_acquire);
 }
 
+int vfrb_dada_set_header(vfrb_dada* d, const char* text, uint64_t n) {
+  if (!d || (!text && n) || n > kHeaderBlock) return VFRB_ERR_ARG;
+  std::memcpy(reinterpret_cast<uint8_t*>(d->h) + kHdrBytes, text, n);
+  d->h->hdr_len.store((uint32_t)n, std::memory_order_release);
+  return VFRB_OK;
+}
+
+int64_t vfrb_dada_get_header(vfrb_dada* d, char* buf, uint64_t cap, int timeout_ms) {
+  if (!d || (!buf && cap)) return -VFRB_ERR_ARG;
+  const double t0 = now_ms();
+  uint32_t n;
+  while ((n = d->h->hdr_len.load(std::memory_order_acquire)) == kNoHeader) {
+    if (now_ms() - t0 > timeout_ms) return -VFRB_ERR_TIMEOUT;
+    nap();
+  }
+  std::memcpy(buf, reinterpret_cast<const uint8_t*>(d->h) + kHdrBytes, n < cap ? n : cap);
+  return (int64_t)n;
+}
+
+int vfrb_dada_iread(const vfrb_dada* d) { return d ? (int)d->h->iread.load(std::memory_order_acquire) : -1; }
+
+int vfrb_dada_force_iread(vfrb_dada* d) {
+  if (!d) return -1;
+  return (int)d->h->iread.exchange(-1, std::memory_order_acq_rel);
+}
+
+int vfrb_dada_open_read(vfrb_dada* d) {
+  if (!d) return VFRB_ERR_ARG;
+  if (d->primary) return VFRB_OK;
+  int32_t none = -1;
+  if (!d->h->iread.compare_exchange_strong(none, d->id, std::memory_order_acq_rel)) return VFRB_ERR;
+  d->primary = true;
+  return VFRB_OK;
+}
+
 int vfrb_dada_close(vfrb_dada* d) {
   if (!d) return VFRB_ERR_ARG;
+  if (d->primary) {  // give the role back unless it was forced away meanwhile
+    int32_t me = d->id;
+    d->h->iread.compare_exchange_strong(me, -1, std::memory_order_acq_rel);
+  }
   if (d->pinned && cudaHostUnregister(d->h) != cudaSuccess) cudaGetLastError();
   munmap(d->h, d->map_bytes);
   delete d;

@@ -64,15 +64,27 @@ struct Source {
     own = f != nullptr;
     return f != nullptr;
   }
-  // ipcio_connect + ipcio_open('R'): waits (bounded) for the writer's ring
-  bool connect(uint32_t key, int wait_ms = 30000) {
+  // ipcio_connect, then the reference's iread force and ipcio_open('R')
+  // (STATS:284-298, TS:357-372) with its log lines; waits (bounded) for the
+  // writer's ring.  Returns 0, 1 (could not connect) or 2 (could not open
+  // as the primary reader).
+  int connect(uint32_t key, FILE* log, int wait_ms = 30000) {
     const double t0 = now_s();
     while (vfrb_dada_connect(key, &ring) != VFRB_OK) {
-      if ((now_s() - t0) * 1e3 > wait_ms) return false;
+      if ((now_s() - t0) * 1e3 > wait_ms) return 1;
       usleep(20000);
     }
+    // iread = -1 is required to open as the primary read client
+    const int iread = vfrb_dada_iread(ring);
+    if (iread != -1) {
+      std::fprintf(log, " iread= %d != -1, setting to -1\n", iread);
+      vfrb_dada_force_iread(ring);
+    } else {
+      std::fprintf(log, " iread= %d, do not need to force\n", iread);
+    }
+    if (vfrb_dada_open_read(ring) != VFRB_OK) return 2;
     pinned = vfrb_dada_pin(ring) == VFRB_OK;  // else pushes go through the staging copy
-    return true;
+    return 0;
   }
   // ring input: the next contiguous readable bytes in place (0 at end of data)
   size_t acquire(const uint8_t** p, size_t max_n) {

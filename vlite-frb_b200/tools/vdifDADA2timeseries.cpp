@@ -186,8 +186,13 @@ int main(int argc, char** argv) {
     }
   } else {
     std::fprintf(log, " Connecting to DADA buffer with key: %x ...\n", key);
-    if (!src.connect(key)) {
+    const int cst = src.connect(key, log);
+    if (cst == 1) {
       std::fprintf(log, " Could not connect to DADA buffer!\n");
+      return 255;  // the reference returns -1
+    }
+    if (cst == 2) {
+      std::fprintf(log, " Could not open for reading DADA buffer!\n");
       return 255;
     }
   }

@@ -4,8 +4,9 @@
 //
 //   vfrb_dada_write -k KEY -i FILE [-cap BYTES] [-chunk BYTES] [-timeout S]
 //
-// Creates the ring (capacity a power of two, default 256 MiB), writes the
-// file, marks end of data, waits (bounded) until the reader has taken every
+// Creates the ring (capacity a power of two, default 256 MiB), sets its
+// header block (DADA-style "KEY value" lines: header version and size, the
+// source file, the VDIF frame geometry), writes the file, marks end of data, waits (bounded) until the reader has taken every
 // byte, and removes the ring.  Exit 0 on success, 2 on an I/O error, 3 when
 // the reader stalled past the timeout.
 #include "tool_common.h"
@@ -43,6 +44,12 @@ int main(int argc, char** argv) {
     std::fprintf(stderr, "cannot create ring %x: %s\n", key, vfrb_strerror(st));
     return 2;
   }
+  char hdr[1024];
+  const int hn = std::snprintf(hdr, sizeof hdr,
+                               "HDR_VERSION 1.0\nHDR_SIZE 4096\nFILE_NAME %s\nENCODING VDIF\nFRAME_SIZE 5032\n"
+                               "NPOL 2\nNBIT 8\nBW 64\nTSAMP 0.0078125\n",
+                               in.c_str());
+  vfrb_dada_set_header(ring, hdr, (uint64_t)std::min(hn, (int)sizeof hdr - 1));
   std::vector<uint8_t> buf((size_t)chunk);
   int rc = 0;
   for (;;) {
