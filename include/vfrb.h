@@ -345,6 +345,13 @@ typedef struct vfrb_params {
                                     * mode, FP32 storage only                 */
   int32_t zero_dm;                 /* 1: subtractZERO after the bandpass
                                     * (PIPE:1478); block mode, FP32 only      */
+  int32_t batch_streams;           /* stream mode: 1 = the dedispersion of the
+                                    * chunks that become ready in several
+                                    * streams runs as one launch (up to 32
+                                    * streams), issued at the next vfrb_poll
+                                    * or when a stream needs its buffers
+                                    * again; results are identical to
+                                    * per-stream launches                  */
 } vfrb_params;
 
 #define VFRB_BP_CAL 0

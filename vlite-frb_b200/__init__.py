@@ -361,7 +361,7 @@ class Params(C.Structure):
                 ("fb_block", C.c_int32), ("nstreams", C.c_int32), ("chunk_seconds", C.c_float),
                 ("ring_seconds", C.c_float), ("cand_snr", C.c_float), ("device", C.c_int32),
                 ("device_bytes", C.c_int64), ("boxcar_max", C.c_int32), ("bp_mode", C.c_int32),
-                ("zero_dm", C.c_int32)]
+                ("zero_dm", C.c_int32), ("batch_streams", C.c_int32)]
 
 
 class Cand(C.Structure):

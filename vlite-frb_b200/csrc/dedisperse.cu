@@ -551,7 +551,7 @@ static int reg_launch(const vfrb_ddplan* pl, int v, const vfrb_dd_args& a, DmPar
 
 template <typename T, int D, int TT, int SMAX, int W>
 static int pat_launch_t(const vfrb_ddplan* pl, const RegGroup& g, const vfrb_dd_args& a, DmPartial* part,
-                        float out_scale, cudaStream_t s, int* ntb) {
+                        float out_scale, cudaStream_t s, int* ntb, const DdJob* jobs = nullptr, int njobs = 0) {
   constexpr int VEC = 16 / (int)sizeof(T);
   constexpr int NT = 32 * TT;
   *ntb = 0;
@@ -590,6 +590,8 @@ static int pat_launch_t(const vfrb_ddplan* pl, const RegGroup& g, const vfrb_dd_
   k.chunk = chunk;
   k.lmax = lm;
   k.err = a.d_err;
+  k.njobs = njobs;
+  for (int i = 0; i < njobs; ++i) k.jobs[i] = jobs[i];
   const size_t meta = 16 + ((size_t)3 * W * chunk + W + 3) / 4 * 16;
   const size_t smem = meta + (size_t)2 * chunk * lm * sizeof(T);
   cudaError_t e =
@@ -600,7 +602,7 @@ static int pat_launch_t(const vfrb_ddplan* pl, const RegGroup& g, const vfrb_dd_
   // channel (see the kernel); the first and last rows hold empty CTAs
   const long long ny = ntime + mid_max / NT;
   if (ny > 65535) return VFRB_OK;
-  dim3 grid((unsigned)nblocks, (unsigned)ny);
+  dim3 grid((unsigned)nblocks, (unsigned)ny, (unsigned)std::max(1, njobs));
   k_dedisp_pat<T, D, TT, SMAX, W><<<grid, W * 32, smem, s>>>(k);
   const int st = cuda_status(cudaGetLastError());
   if (st == VFRB_OK) *ntb = (int)ntime;
@@ -609,7 +611,7 @@ static int pat_launch_t(const vfrb_ddplan* pl, const RegGroup& g, const vfrb_dd_
 
 // Pattern-run variant `v` for this call; *ntb == 0 when it does not apply.
 static int pat_launch(const vfrb_ddplan* pl, int v, const vfrb_dd_args& a, DmPartial* part, cudaStream_t s,
-                      int* ntb) {
+                      int* ntb, const DdJob* jobs = nullptr, int njobs = 0) {
   *ntb = 0;
   if (((uintptr_t)a.fb & 15) != 0) return VFRB_OK;
   const int D = v == VFRB_DD_PAT4 ? 4 : 2;
@@ -621,14 +623,15 @@ static int pat_launch(const vfrb_ddplan* pl, int v, const vfrb_dd_args& a, DmPar
     // between twice as many trials (48.9 vs 55.2 ms at the 61,440-sample x
     // 2048-trial shape); FP16 tiles are half the size, and there the 8-warp
     // form is faster (47.7 vs 49.3 ms)
-    if (D == 4) return pat_launch_t<float, 4, 15, VFRB_PAT4_SMAX, 16>(pl, *g, a, part, 1.f, s, ntb);
-    return pat_launch_t<float, 2, 27, VFRB_PAT2_SMAX, 8>(pl, *g, a, part, 1.f, s, ntb);
+    if (D == 4) return pat_launch_t<float, 4, 15, VFRB_PAT4_SMAX, 16>(pl, *g, a, part, 1.f, s, ntb, jobs, njobs);
+    return pat_launch_t<float, 2, 27, VFRB_PAT2_SMAX, 8>(pl, *g, a, part, 1.f, s, ntb, jobs, njobs);
   }
   if (a.storage == VFRB_F16) {
     if (a.chan_scale || !(a.uniform_scale > 0.f)) return VFRB_OK;
     if (a.chan_stride % 8 || ((unsigned long long)a.row_mask + 1ULL) % 8) return VFRB_OK;
-    if (D == 4) return pat_launch_t<__half, 4, 14, VFRB_PAT4_SMAX, 8>(pl, *g, a, part, a.uniform_scale, s, ntb);
-    return pat_launch_t<__half, 2, 26, VFRB_PAT2_SMAX, 8>(pl, *g, a, part, a.uniform_scale, s, ntb);
+    if (D == 4)
+      return pat_launch_t<__half, 4, 14, VFRB_PAT4_SMAX, 8>(pl, *g, a, part, a.uniform_scale, s, ntb, jobs, njobs);
+    return pat_launch_t<__half, 2, 26, VFRB_PAT2_SMAX, 8>(pl, *g, a, part, a.uniform_scale, s, ntb, jobs, njobs);
   }
   return VFRB_OK;
 }
@@ -714,6 +717,44 @@ int launch_dedisperse_plan(const vfrb_ddplan* pl, const vfrb_dd_args& a, cudaStr
   int v = pl->variant[a.storage];
   if (v == VFRB_DD_AUTO) v = default_variant(pl, a.storage);
   return launch_variant(pl, v, a, s);
+}
+
+// One launch of the pattern kernel over several streams' chunks (grid z =
+// job), the series only (no statistics partials).  Every job shares the
+// plan's delay tables and the ring geometry (chan_stride, row_mask); the
+// launch covers the longest job, the other jobs' surplus CTAs return at
+// once.  *launched = 0 when the plan's kernel for this storage form is not
+// a pattern kernel (or does not apply): the caller then dedisperses the
+// jobs one by one.
+int launch_dedisperse_jobs(const vfrb_ddplan* pl, int storage, const DdJob* jobs, int njobs, long long chan_stride,
+                           unsigned row_mask, cudaStream_t s, int* launched) {
+  *launched = 0;
+  if (!pl || njobs < 1 || njobs > kDdMaxJobs || storage < VFRB_F32 || storage > VFRB_F16) return VFRB_ERR_ARG;
+  int v = pl->variant[storage];
+  if (v == VFRB_DD_AUTO) v = default_variant(pl, storage);
+  if (v != VFRB_DD_PAT4 && v != VFRB_DD_PAT2) return VFRB_OK;
+  vfrb_dd_args a{};
+  a.fb = jobs[0].fb;
+  a.storage = storage;
+  a.uniform_scale = storage == VFRB_F16 ? jobs[0].out_scale : 0.f;
+  a.chan_stride = chan_stride;
+  a.row_mask = row_mask;
+  a.nrows_valid = jobs[0].nrows_valid;
+  long long nt = 0;
+  for (int i = 0; i < njobs; ++i) {
+    nt = std::max(nt, jobs[i].nt_out);
+    if (((uintptr_t)jobs[i].fb & 15) != 0 || (storage == VFRB_F16 && !(jobs[i].out_scale > 0.f)) ||
+        jobs[i].nrows_valid < jobs[i].nt_out + pl->max_delay)
+      return VFRB_OK;
+  }
+  a.nt_out = nt;
+  a.out = jobs[0].out;
+  a.out_stride = jobs[0].out_stride;
+  int ntb = 0;
+  const int st = pat_launch(pl, v, a, nullptr, s, &ntb, jobs, njobs);
+  if (st) return st;
+  *launched = ntb > 0;
+  return VFRB_OK;
 }
 
 // Time every applicable variant on scratch data and keep the fastest.

@@ -29,7 +29,10 @@ namespace vfrb {
 constexpr int kPatWarps = 8;  // warps per CTA of the two-CTAs-per-SM form (the other: 16, one CTA)
 constexpr unsigned char kPatGeneric = 255;
 
+
 struct DdPatParams {
+  int njobs;                   // 0: one launch with the fields below; else jobs[blockIdx.z] overrides them
+  DdJob jobs[kDdMaxJobs];
   const void* fb;
   float out_scale;  // multiplies sum/nchan (1 for FP32, S for FP16)
   long long chan_stride;
@@ -205,7 +208,41 @@ __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, unsigned by
 // W warps per CTA: 8 (two CTAs per SM, ~110 KB of tiles each) or 16 (one
 // CTA per SM sharing ~220 KB of tiles between twice as many DM trials)
 template <typename T, int D, int TT, int SMAX, int W>
-__global__ void __launch_bounds__(W * 32, 16 / W) k_dedisp_pat(const DdPatParams p) {
+__global__ void __launch_bounds__(W * 32, 16 / W) k_dedisp_pat(const DdPatParams pp) {
+  // a batched launch: this CTA's stream's fields from its job
+  DdPatParams p;
+  p.fb = pp.fb;
+  p.out_scale = pp.out_scale;
+  p.row0 = pp.row0;
+  p.nrows_valid = pp.nrows_valid;
+  p.nt_out = pp.nt_out;
+  p.out = pp.out;
+  p.out_stride = pp.out_stride;
+  p.err = pp.err;
+  p.part = pp.part;
+  if (pp.njobs > 0) {
+    const DdJob& j = pp.jobs[blockIdx.z];
+    p.fb = j.fb;
+    p.out_scale = j.out_scale;
+    p.row0 = j.row0;
+    p.nrows_valid = j.nrows_valid;
+    p.nt_out = j.nt_out;
+    p.out = j.out;
+    p.out_stride = j.out_stride;
+    p.err = j.err;
+    p.part = nullptr;  // batched launches are stream mode: statistics come from the series
+  }
+  p.chan_stride = pp.chan_stride;
+  p.row_mask = pp.row_mask;
+  p.nchan = pp.nchan;
+  p.ndm = pp.ndm;
+  p.ngroups = pp.ngroups;
+  p.gbase = pp.gbase;
+  p.gpack = pp.gpack;
+  p.gpat = pp.gpat;
+  p.bmin = pp.bmin;
+  p.chunk = pp.chunk;
+  p.lmax = pp.lmax;
   constexpr int VEC = 16 / (int)sizeof(T);
   constexpr int NT = 32 * TT;
   static_assert(sizeof(T) == 4 ? (TT & 1) == 1 : (TT & 3) == 2, "lane stride must spread loads over all banks");

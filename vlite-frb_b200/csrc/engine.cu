@@ -214,6 +214,12 @@ struct StreamSt {
   int64_t rows_chan = 0, rows_bp = 0, rows_out = 0;
   int64_t chunks = 0;
   int64_t stat_blocks = 0;     // TIMESTATS blocks emitted (VFRB_OUT_CHANSTATS)
+  // batch_streams: chunks whose dedispersion waits for the plan's shared
+  // launch (rows, output chunks, and when their data were complete)
+  bool job = false;
+  int64_t job_row0 = 0, job_nvalid = 0, job_k = 0, job_nt = 0, job_seq0 = 0;
+  double job_t_push = 0.0;
+  cudaEvent_t ev_ready = nullptr;
   // both
   void* d_cm = nullptr;  // channel-major bandpassed FB (storage form)
   int64_t cm_stride = 0;
@@ -255,6 +261,11 @@ struct vfrb_plan {
   std::deque<ResultSlot*> queue;  // submission order
   ResultSlot* held = nullptr;     // returned by the last poll
   std::string logtmp;
+  // stream mode, batch_streams: streams whose chunks wait for one shared
+  // dedispersion launch on bs
+  std::vector<StreamSt*> pending;
+  cudaStream_t bs = nullptr;
+  cudaEvent_t ev_batch = nullptr;
 };
 
 namespace {
@@ -548,7 +559,8 @@ int run_bandpass(vfrb_plan* pl, StreamSt* s, const float* raw, int64_t in_row0, 
 // Dedisperse nt samples into d_out.  kernel_stats: calcstats (and the boxcar
 // search) of the whole launch, fused (block mode); otherwise each output
 // chunk gets its statistics from chunk_stats (stream mode).
-int run_dedisp(vfrb_plan* pl, StreamSt* s, int64_t row0, int64_t nrows_valid, int64_t nt, bool kernel_stats) {
+int run_dedisp(vfrb_plan* pl, StreamSt* s, int64_t row0, int64_t nrows_valid, int64_t nt, bool kernel_stats,
+               cudaStream_t on = nullptr) {
   const Range nvtx_range("vfrb dedisperse");
   vfrb_dd_args a{};
   a.fb = s->d_cm;
@@ -572,7 +584,7 @@ int run_dedisp(vfrb_plan* pl, StreamSt* s, int64_t row0, int64_t nrows_valid, in
   a.frb = stats ? s->d_frb : nullptr;
   a.argmax = stats ? s->d_arg : nullptr;
   a.d_err = s->d_err;
-  ST(launch_dedisperse_plan(pl->dd, a, s->cs));
+  ST(launch_dedisperse_plan(pl->dd, a, on ? on : s->cs));
   if (kernel_stats && boxcar_on(pl))
     ST(launch_boxcar(s->d_out, pl->ndm, nt, s->out_stride, s->d_ave, s->d_sgm, pl->P.boxcar_max, s->d_bsnr, s->d_bt,
                      s->d_bw, s->cs));
@@ -580,7 +592,8 @@ int run_dedisp(vfrb_plan* pl, StreamSt* s, int64_t row0, int64_t nrows_valid, in
 }
 
 // Copy this result's outputs to the host and queue it.
-int emit(vfrb_plan* pl, StreamSt* s, int64_t seq, int64_t row0, int64_t nt, bool with_fb, int64_t col0 = 0) {
+int emit(vfrb_plan* pl, StreamSt* s, int64_t seq, int64_t row0, int64_t nt, bool with_fb, int64_t col0 = 0,
+         double t_data = -1.0) {
   ResultSlot* r = nullptr;
   ST(alloc_slot(pl, s, &r));
   const int64_t nch = pl->L.nchanout;
@@ -656,7 +669,7 @@ int emit(vfrb_plan* pl, StreamSt* s, int64_t seq, int64_t row0, int64_t nt, bool
   o.chan_sk = cst ? r->csk : nullptr;
   o.nflag_rows = (int64_t)r->flags.size();
   o.row_flags = r->flags.empty() ? nullptr : r->flags.data();
-  r->t_data = s->t_push;
+  r->t_data = t_data >= 0.0 ? t_data : s->t_push;
   r->state = 1;
   pl->queue.push_back(r);
   return VFRB_OK;
@@ -794,8 +807,70 @@ int stream_stats_block(vfrb_plan* pl, StreamSt* s, int64_t k) {
 }
 
 // k output chunks of nt samples each with one dedispersion launch
+bool batching(const vfrb_plan* pl) {
+  return pl->P.batch_streams && pl->P.mode == VFRB_MODE_STREAM && !want(pl, VFRB_OUT_SIGMA) && pl->bs;
+}
+
+// The pending streams' chunks dedispersed by one launch on the plan's batch
+// stream (after each stream's bandpass, recorded in its ev_ready), then each
+// stream's per-chunk statistics and results on its own stream after the
+// launch.  Results are the per-stream launch's bit for bit: the same kernel
+// with the same inputs.
+int flush_batch(vfrb_plan* pl) {
+  if (pl->pending.empty()) return VFRB_OK;
+  const Range nvtx_range("vfrb batched dedisperse");
+  std::vector<DdJob> jobs;
+  for (StreamSt* s : pl->pending) {
+    CK(cudaStreamWaitEvent(pl->bs, s->ev_ready, 0));
+    DdJob j{};
+    j.fb = s->d_cm;
+    j.out_scale = pl->P.storage == VFRB_F16 ? s->uscale : 1.f;
+    j.row0 = s->job_row0;
+    j.nrows_valid = s->job_nvalid;
+    j.nt_out = s->job_k * s->job_nt;
+    j.out = s->d_out;
+    j.out_stride = s->out_stride;
+    j.err = s->d_err;
+    jobs.push_back(j);
+  }
+  StreamSt* s0 = pl->pending.front();
+  int launched = 0;
+  ST(launch_dedisperse_jobs(pl->dd, pl->P.storage, jobs.data(), (int)jobs.size(), s0->cm_stride, s0->cm_mask, pl->bs,
+                            &launched));
+  if (!launched)  // the plan's kernel has no batched form: one launch per stream, on the batch stream
+    for (StreamSt* s : pl->pending) ST(run_dedisp(pl, s, s->job_row0, s->job_nvalid, s->job_k * s->job_nt, false, pl->bs));
+  CK(cudaEventRecord(pl->ev_batch, pl->bs));
+  std::vector<StreamSt*> done;
+  done.swap(pl->pending);
+  for (StreamSt* s : done) {
+    CK(cudaStreamWaitEvent(s->cs, pl->ev_batch, 0));
+    for (int64_t i = 0; i < s->job_k; ++i) {
+      ST(chunk_stats(pl, s, i * s->job_nt, s->job_nt));
+      ST(emit(pl, s, s->job_seq0 + i, s->job_row0 + i * s->job_nt, s->job_nt, false, i * s->job_nt, s->job_t_push));
+    }
+    s->job = false;
+  }
+  return VFRB_OK;
+}
+
 int stream_chunks(vfrb_plan* pl, StreamSt* s, int64_t k, int64_t nt) {
   const Range nvtx_range("vfrb stream chunks");
+  if (batching(pl)) {
+    // a stream's output buffer holds one job: a second one waits for the first's launch
+    if (s->job || (int)pl->pending.size() >= kDdMaxJobs) ST(flush_batch(pl));
+    CK(cudaEventRecord(s->ev_ready, s->cs));
+    s->job = true;
+    s->job_row0 = s->rows_out;
+    s->job_nvalid = s->rows_bp - s->rows_out;
+    s->job_k = k;
+    s->job_nt = nt;
+    s->job_seq0 = s->chunks;
+    s->job_t_push = s->t_push;
+    s->rows_out += k * nt;
+    s->chunks += k;
+    pl->pending.push_back(s);
+    return VFRB_OK;
+  }
   ST(run_dedisp(pl, s, s->rows_out, s->rows_bp - s->rows_out, k * nt, false));
   for (int64_t i = 0; i < k; ++i) {
     ST(chunk_stats(pl, s, i * nt, nt));
@@ -846,10 +921,14 @@ int process(vfrb_plan* pl, StreamSt* s, bool final_flush) {
     s->rows_chan += n;
     consume_entries(s, (s->rows_chan * S) / kDataLen);
     const int64_t w1 = (s->rows_chan / 128) * 128;
+    // a pending job's rows stay in the channel-major ring until its launch
+    if (s->job && w1 > s->job_row0 + (int64_t)s->cm_mask + 1) ST(flush_batch(pl));
     if (w1 > s->rows_bp) {
       ST(run_bandpass(pl, s, s->d_raw, s->rows_bp, (unsigned)(s->R1 - 1), w1 - s->rows_bp, s->rows_bp, nullptr));
       s->rows_bp = w1;
     }
+    // statistics results stay after the stream's earlier series results
+    if (stats && s->job && (s->stat_blocks + 1) * pl->ncolstatblk <= s->rows_bp) ST(flush_batch(pl));
     while (stats && (s->stat_blocks + 1) * pl->ncolstatblk <= s->rows_bp) {
       ST(stream_stats_block(pl, s, s->stat_blocks));
       ++s->stat_blocks;
@@ -995,6 +1074,11 @@ int free_plan(vfrb_plan* pl) {
   if (!pl) return VFRB_OK;
   for (auto& s : pl->st)
     if (s) s->res.release();
+  if (pl->bs) {
+    cudaStreamSynchronize(pl->bs);
+    cudaStreamDestroy(pl->bs);
+  }
+  if (pl->ev_batch) cudaEventDestroy(pl->ev_batch);
   if (pl->dd) ddplan_destroy(pl->dd);
   delete pl;
   return VFRB_OK;
@@ -1016,6 +1100,7 @@ int create_stream(vfrb_plan* pl, int id, int64_t ring_frames, int64_t R1, int64_
   ST(mkstream(s->res, &s->hs));
   ST(mkevent(s->res, &s->ev_copied));
   ST(mkevent(s->res, &s->ev_consumed));
+  ST(mkevent(s->res, &s->ev_ready));
   for (auto& e : s->rel_ev) ST(mkevent(s->res, &e));
   CK(cudaEventRecord(s->ev_consumed, s->cs));
   s->ring_frames = ring_frames;
@@ -1236,6 +1321,13 @@ int vfrb_plan_create(vfrb_plan** out, const vfrb_params* prm) {
   if (cudaMemGetInfo(&fr, &tot) != cudaSuccess) return fail(VFRB_ERR_CUDA);
   const int64_t budget = P.device_bytes > 0 ? P.device_bytes : (int64_t)(0.9 * (double)fr);
   if (need > budget) return fail(VFRB_ERR_NOMEM);
+  if (P.batch_streams && P.mode == VFRB_MODE_STREAM) {
+    if (cudaStreamCreateWithFlags(&pl->bs, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&pl->ev_batch, cudaEventDisableTiming) != cudaSuccess) {
+      cudaGetLastError();
+      return fail(VFRB_ERR_CUDA);
+    }
+  }
   for (int i = 0; i < P.nstreams; ++i) {
     st = create_stream(pl, i, ring_frames, R1, R2);
     if (st) return fail(st);
@@ -1327,6 +1419,7 @@ int vfrb_push_frames(vfrb_plan* pl, int stream, const uint8_t* bytes, size_t nby
     s->reader->end_of_data();
     ST(run_reader(pl, s));
     ST(process(pl, s, true));
+    ST(flush_batch(pl));
     s->ended = true;
     return s->reader_error;
   }
@@ -1369,6 +1462,7 @@ int vfrb_poll(vfrb_plan* pl, vfrb_result* out, int wait) {
     pl->held->state = 0;
     pl->held = nullptr;
   }
+  ST(flush_batch(pl));  // the chunks that became ready since the last poll, as one launch
   if (pl->queue.empty()) {
     for (auto& s : pl->st)
       if (s && !s->ended && !s->reader_error) return VFRB_PENDING;  // a failed stream produces nothing more

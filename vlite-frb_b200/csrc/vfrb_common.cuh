@@ -24,6 +24,22 @@ constexpr int kErrTimeout = 8;       // a bounded device wait gave up
 
 inline int cuda_status(cudaError_t e) { return e == cudaSuccess ? VFRB_OK : VFRB_ERR_CUDA; }
 
+// One stream's share of a batched dedispersion launch (grid z = job): what
+// differs between streams of a plan -- their filterbank ring, FP16 scale,
+// rows and output.  The delay tables, ring geometry and trial grid are the
+// plan's.
+struct DdJob {
+  const void* fb;
+  float out_scale;
+  long long row0;
+  long long nrows_valid;
+  long long nt_out;
+  float* out;
+  long long out_stride;
+  int* err;
+};
+constexpr int kDdMaxJobs = 32;
+
 // Launchers (host side, defined in the .cu files).
 int launch_channelise(const vfrb_chan_args& a, cudaStream_t s);
 int launch_bandpass(const vfrb_bp_args& a, cudaStream_t s);
@@ -38,5 +54,10 @@ int launch_subtract_bp_full(float* fb, long long chan_stride, long long row0, un
                             long long nrows, cudaStream_t s);
 int launch_subtract_zero(float* fb, long long chan_stride, long long row0, unsigned row_mask, int nchan,
                          long long nrows, cudaStream_t s);
+}  // namespace vfrb
+struct vfrb_ddplan;
+namespace vfrb {
+int launch_dedisperse_jobs(const vfrb_ddplan* pl, int storage, const DdJob* jobs, int njobs, long long chan_stride,
+                           unsigned row_mask, cudaStream_t s, int* launched);
 
 }  // namespace vfrb
