@@ -80,8 +80,8 @@ def full60(vf, O):
     del rows
     cm = co.transpose(bp)
     del bp
-    off, md_o = O.delay_table(dms, L.fch1, L.chanbw, L.tchan, L.nchanout)
-    assert md_o == md
+    off, _ = O.delay_table(dms, L.fch1, L.chanbw, L.tchan, L.nchanout)
+    assert int(off.max()) == md  # stream mode carries the table's largest delay
     dd = co.dedisperse_cm(cm, off, nbp - md)
     del cm
     t_oracle = time.perf_counter() - t0

@@ -494,7 +494,7 @@ class Plan:
             return r
         ndm, nt, nch = r.ndm, r.nt, r.nchan
         out = dict(stream=r.stream, seq=r.seq, row0=r.row0, tstart_mjd=r.tstart_mjd, ndm=ndm, nt=nt,
-                   latency_ms=r.latency_ms, device_errors=r.device_errors)
+                   latency_ms=r.latency_ms, device_errors=r.device_errors, nstatblks=r.nstatblks)
         dd = _arr(r.dd, ndm * nt, C.c_float)
         out["dd"] = dd.reshape(ndm, nt) if dd is not None else None
         ds = _arr(r.dd_sigma, ndm * nt, C.c_float)
