@@ -27,7 +27,14 @@
 // One persistent 256-thread CTA per SM (a radix-25 pol-pair butterfly holds
 // 100 floats, so a thread needs up to 255 registers).  The raw bytes of the
 // next window are copied from the frame ring into a shared-memory byte buffer
-// with 4-byte cp.async while the current window is transformed.
+// with 4-byte cp.async while the current window is transformed.  The copies
+// are issued by warps 2..7 only: pass 3 has 313 tasks for 256 threads, and
+// the 57 second-round tasks of warps 0 and 1 run while the other six warps
+// issue the copies (payload pieces with one source pointer each, so a copy
+// costs a few instructions).  Frames sit 5032 bytes apart in the frame ring
+// and a payload is 5000 bytes, both 8 mod 16, so the pieces of one window
+// differ in alignment mod 16 and no single shared-memory offset makes every
+// piece a legal 16-byte or bulk copy.
 #include "vfrb_common.cuh"
 #include "dft_pairs.cuh"
 
@@ -43,6 +50,10 @@ constexpr int kPB = kH / 25;           // 250 butterflies in passes 1 and 2
 constexpr int kPM3 = kH / 10;          // 625 butterflies in pass 3
 constexpr int kPTasks = kPM3 / 2 + 1;  // 313 pass-3 tasks: pairs (j, 625 - j), and j = 0
 constexpr int kStage = 12512;          // one pol's window bytes, padded to 16
+// the staging copies are issued by warps 2..7: pass 3's second round (threads
+// 0..56) then runs while they copy
+constexpr int kStageT0 = 64;
+constexpr int kStageThreads = kPThreads - kStageT0;
 
 // Twiddle tables, as (c, c, s, s) so a twiddle is one packed pair per
 // component, computed on the host in double precision:
@@ -138,31 +149,48 @@ __device__ __forceinline__ PolPair pp_from_word(unsigned w) {
 template <bool ALIGNED>
 __device__ __forceinline__ void pp_stage(unsigned char* __restrict__ st0, unsigned char* __restrict__ st1,
                                          const vfrb_chan_args& a, long long pos0, int& err) {
-  const int tid = threadIdx.x;
+  const int tid = (int)threadIdx.x - kStageT0;  // staging thread index
+  if (tid < 0) return;
   if (ALIGNED) {
+    // the window's bytes [0, 12500) start at payload offset off0 of slot
+    // slot0 and cover up to 4 payload pieces; the pieces' slot entries are
+    // loaded together, then each piece is copied from one source pointer
     const long long slot0 = pos0 >= 0 ? pos0 / kDataLen : -1;
     const int off0 = pos0 >= 0 ? (int)(pos0 - slot0 * kDataLen) : 0;
-    for (int g = tid; g < kFftN / 4; g += kPThreads) {
-      const int o = off0 + 4 * g;  // < 5000 + 12500
-      const int q = o / kDataLen;
+    long long sv0[4], sv1[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
       const long long slot = slot0 + q;
-      const int off = o - q * kDataLen;
-      long long s0 = -1, s1 = -1;
-      if (slot0 < 0 || slot >= a.nslots) {
+      const bool in = slot0 >= 0 && slot < a.nslots && q * kDataLen - off0 < kFftN;
+      sv0[q] = in ? __ldg(a.slots0 + slot) : -1;
+      sv1[q] = in ? __ldg(a.slots1 + slot) : -1;
+      if (!in && q * kDataLen - off0 < kFftN) err |= kErrSlotRange;
+    }
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int lo = max(0, q * kDataLen - off0), hi = min(kFftN, (q + 1) * kDataLen - off0);
+      long long s0 = sv0[q], s1 = sv1[q];
+      if ((s0 >= 0 && (s0 & 3)) || (s1 >= 0 && (s1 & 3))) {  // payloads must start on a 4-byte boundary
         err |= kErrSlotRange;
-      } else {
-        s0 = __ldg(a.slots0 + slot);
-        s1 = __ldg(a.slots1 + slot);
-        if ((s0 >= 0 && (s0 & 3)) || (s1 >= 0 && (s1 & 3))) {  // payloads must start on a 4-byte boundary
-          err |= kErrSlotRange;
-          s0 = s1 = -1;
-        }
+        s0 = s1 = -1;
       }
-      cp_async4(st0 + 4 * g, s0 >= 0 ? a.frames + s0 + off : a.frames, s0 >= 0 ? 4 : 0);
-      cp_async4(st1 + 4 * g, s1 >= 0 ? a.frames + s1 + off : a.frames, s1 >= 0 ? 4 : 0);
+      // window byte n of this piece is payload byte n + off0 - q * kDataLen
+      const long long d = (long long)off0 - (long long)q * kDataLen;
+      const int n0 = s0 >= 0 ? 4 : 0, n1 = s1 >= 0 ? 4 : 0;  // source bytes (0: zero fill)
+      const int glo = lo / 4, ghi = hi / 4;
+      int g = glo + ((tid - glo) % kStageThreads + kStageThreads) % kStageThreads;
+      const unsigned char* q0 = s0 >= 0 ? a.frames + s0 + d + 4LL * g : a.frames;
+      const unsigned char* q1 = s1 >= 0 ? a.frames + s1 + d + 4LL * g : a.frames;
+      const int m0 = n0 * kStageThreads, m1 = n1 * kStageThreads;  // source step per copy (0 when zero filling)
+      for (; g < ghi; g += kStageThreads) {
+        cp_async4(st0 + 4 * g, q0, n0);
+        cp_async4(st1 + 4 * g, q1, n1);
+        q0 += m0;
+        q1 += m1;
+      }
     }
   } else {
-    for (int n = tid; n < kFftN; n += kPThreads) {
+    for (int n = tid; n < kFftN; n += kStageThreads) {
       const long long pos = pos0 + n;
       const long long slot = pos >= 0 ? pos / kDataLen : -1;
       unsigned char v0 = 0, v1 = 0;
