@@ -48,12 +48,11 @@ def _run(cmd):
 
 def gen_codelets():
     gen = os.path.join(CSRC, "gen_dft.py")
-    for name, flags in (("dft_codelets.cuh", []), ("dft_pairs.cuh", ["--pairs"])):
-        out = os.path.join(CSRC, name)
-        if _newer(gen, out):
-            txt = subprocess.run([sys.executable, gen, *flags], capture_output=True, text=True, check=True).stdout
-            with open(out, "w") as f:
-                f.write(txt)
+    out = os.path.join(CSRC, "dft_pairs.cuh")
+    if _newer(gen, out):
+        txt = subprocess.run([sys.executable, gen], capture_output=True, text=True, check=True).stdout
+        with open(out, "w") as f:
+            f.write(txt)
     pat = os.path.join(CSRC, "gen_patterns.py")
     if _newer(pat, os.path.join(CSRC, "dedisp_patterns.cuh")):
         subprocess.run([sys.executable, pat], check=True)

@@ -1,4 +1,4 @@
-// Generated by gen_dft.py --pairs -- do not edit by hand.
+// Generated by gen_dft.py -- do not edit by hand.
 // Forward DFT codelets (W = exp(-2*pi*i/N)) on pairs of polarisations: a
 // PolPair holds one complex sample of pol 0 and pol 1 as re = (re0, re1),
 // im = (im0, im1), so each step is one packed FP32 instruction (sm_100).
