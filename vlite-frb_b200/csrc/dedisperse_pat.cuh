@@ -80,10 +80,25 @@ struct PatMax<A> {
 };
 
 // acc[J + i][t] += w[t + S_i] for the trials J, J+1, ... with shifts S...
+// FP32 with an even shift: the samples t, t + 1 (t even) and the window
+// elements t + S, t + S + 1 are both register pairs, so one packed add
+// (add.rn.f32x2, two independent round-to-nearest adds: the same results as
+// two scalar adds) serves two samples.  An odd shift would pair elements
+// across register pairs and stays scalar.
 template <typename T, int D, int TT, int NW, int J, int S0, int... SR>
 __device__ __forceinline__ void pat_add(float (&acc)[D][TT], const typename PatElem<T>::R (&w)[NW]) {
+  if constexpr (sizeof(T) == 4 && (S0 & 1) == 0) {
 #pragma unroll
-  for (int t = 0; t < TT; ++t) acc[J][t] = PatElem<T>::add(acc[J][t], w[t + S0]);
+    for (int t = 0; t + 1 < TT; t += 2) {
+      const float2 r = __fadd2_rn(make_float2(acc[J][t], acc[J][t + 1]), make_float2(w[t + S0], w[t + S0 + 1]));
+      acc[J][t] = r.x;
+      acc[J][t + 1] = r.y;
+    }
+    if constexpr ((TT & 1) != 0) acc[J][TT - 1] = acc[J][TT - 1] + w[TT - 1 + S0];
+  } else {
+#pragma unroll
+    for (int t = 0; t < TT; ++t) acc[J][t] = PatElem<T>::add(acc[J][t], w[t + S0]);
+  }
   if constexpr (sizeof...(SR) > 0) pat_add<T, D, TT, NW, J + 1, SR...>(acc, w);
 }
 
