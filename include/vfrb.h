@@ -436,7 +436,10 @@ int64_t vfrb_plan_device_bytes(const vfrb_plan* plan);
  * staging buffer; `bytes` may also be device memory of the plan's device
  * (frames already on the GPU, e.g. from a capture kernel): they are copied
  * device to device and only their 32-byte headers go to the host for the
- * pair reader.  `bytes` may be reused as soon as the call returns. */
+ * pair reader.  Device input is read after all work queued before the call
+ * on the legacy default stream (PyTorch's default stream); input written on
+ * another stream must be complete (that stream synchronised) before the
+ * call.  `bytes` may be reused as soon as the call returns. */
 int vfrb_push_frames(vfrb_plan* plan, int stream, const uint8_t* bytes, size_t nbytes);
 
 /* Streams opened and closed while others run (serving).  vfrb_stream_open

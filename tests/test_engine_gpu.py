@@ -470,6 +470,52 @@ def test_stream_device_input_matches_host(vf):
         assert np.array_equal(x["row_flags"], y["row_flags"]) and x["device_errors"] == y["device_errors"] == 0
 
 
+def test_stream_device_input_ordered_after_producer(vf):
+    """Device chunks pushed the moment the kernels that write them are queued
+    (on PyTorch's default stream, no synchronisation) are read only after
+    those kernels: results equal the same chunks pushed from pinned host
+    copies, bit for bit, with cuts anywhere.  12 s of one stream in chunks of
+    0.5-4 s (device batches of a quarter of the 1-s frame ring), statistics
+    blocks, the zero-DM series and its sigma, row flags."""
+    import torch
+    from vlite_frb_b200 import synth
+    rng = np.random.default_rng(3)
+    fps, total, sched, pos = 25600, 12 * 25600, [], 0
+    while pos < total:
+        n = min(total - pos, int(rng.uniform(0.5, 4.0) * fps) // 5 * 5)
+        sched.append((pos, n))
+        pos += n
+    cuts = [sorted(set([0, n * 10064] + [int(x) for x in rng.integers(1, n * 10064, 2)])) for _, n in sched]
+
+    def run(pinned):
+        plan = vf.Plan(np.zeros(1, np.float32), nave=4, mode=vf.MODE_STREAM, chunk_seconds=1.0, ring_seconds=1.0,
+                       timestats=1.0, outputs=vf.OUT_CHANSTATS | vf.OUT_DEDISP | vf.OUT_SIGMA | vf.OUT_FLAGS)
+        res = []
+        for k, (p0, n) in enumerate(sched):
+            spec = synth.StreamSpec(duration=n / fps, seed=900 + k, frame0=p0, block0=p0 * 5000 // 12500,
+                                    rfi=synth.Rfi(seed=9))
+            fr = synth.make_vdif(spec, device="cuda")
+            if pinned:
+                h = torch.empty(fr.numel(), dtype=torch.uint8, pin_memory=True)
+                h.copy_(fr)
+                fr = h
+            for a, b in zip(cuts[k][:-1], cuts[k][1:]):
+                plan.push(0, fr[a:b])
+            while (r := plan.poll(wait=False)) is not None:
+                res.append(r)
+        plan.push(0, None)
+        res += plan.drain()
+        plan.close()
+        return res
+
+    dev, host = run(False), run(True)
+    assert len(dev) == len(host) > 10
+    for x, y in zip(dev, host):
+        assert (x["row0"], x["nt"], x["nstatblks"]) == (y["row0"], y["nt"], y["nstatblks"])
+        for key in ("dd", "dd_sigma", "chan_ave", "chan_sig", "chan_outlier", "chan_sk", "row_flags"):
+            assert (x[key] is None and y[key] is None) or np.array_equal(x[key], y[key]), key
+
+
 @pytest.mark.parametrize("storage", [0, 1])
 def test_stream_batched_dedispersion_equals_per_stream(vf, storage):
     """batch_streams = 1: the chunks that become ready in several streams are

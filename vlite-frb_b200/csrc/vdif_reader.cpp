@@ -151,14 +151,14 @@ PairReader::Status PairReader::run(std::vector<int64_t>& e0, std::vector<int64_t
 }
 
 size_t PairReader::run_fast(const uint8_t* fr, int64_t pay0, size_t n, std::vector<int64_t>& e0,
-                            std::vector<int64_t>& e1) {
+                            std::vector<int64_t>& e1, size_t pitch) {
   if (phase_ != RUNNING || !q_.empty() || nskip_[0] || nskip_[1]) return 0;
   const bool ts = mode_ == TS;
   size_t k = 0;
   for (; k + 1 < n; k += 2) {
     uint32_t w0[2], w1[2];
     for (int p = 0; p < 2; ++p) {
-      const uint8_t* h = fr + (k + p) * (size_t)kFrameLen;
+      const uint8_t* h = fr + (k + p) * pitch;
       std::memcpy(&w0[p], h, 4);  // seconds:30 | legacy | invalid (little-endian, vdifio.h:53-72)
       std::memcpy(&w1[p], h + 4, 4);  // frame:24 | epoch:6 | unassigned:2
     }
@@ -201,7 +201,7 @@ extern "C" int vfrb_read_pairs(const uint8_t* bytes, size_t nbytes, int reader_m
   // queued for the general state machine
   for (size_t k0 = 0; k0 < nfr && st != PairReader::STEP_ERROR; k0 += per) {
     const size_t k1 = std::min(nfr, k0 + per);
-    size_t k = k0 + r.run_fast(bytes + k0 * kFrameLen, (int64_t)k0, k1 - k0, a, b);
+    size_t k = k0 + r.run_fast(bytes + k0 * kFrameLen, (int64_t)k0, k1 - k0, a, b, kFrameLen);
     for (; k < k1; ++k) {
       QFrame q;
       vfrb_decode_header(bytes + k * kFrameLen, &q.h);

@@ -57,8 +57,10 @@ class PairReader {
   // each frame has the expected frame number (and second, TS), appending
   // their pairs exactly as run() would.  Stops before the first frame that
   // needs the general state machine; returns the frames consumed (even).
+  // Frame k's header starts at frames + k * pitch: the frames themselves
+  // (pitch 5032) or their 32-byte headers packed (pitch 32).
   size_t run_fast(const uint8_t* frames, int64_t pay0, size_t nframes, std::vector<int64_t>& e0,
-                  std::vector<int64_t>& e1);
+                  std::vector<int64_t>& e1, size_t pitch);
 
   bool initialised() const { return phase_ == RUNNING; }
   // header of the first pol-0 frame used (tstart for getVDIFDMJD, PIPE:525)
