@@ -1060,8 +1060,13 @@ int feed_frames(vfrb_plan* pl, StreamSt* s, const uint8_t* in, int64_t nf, MemKi
     CK(cudaEventRecord(s->ev_copied, s->xs));
     CK(cudaStreamWaitEvent(s->cs, s->ev_copied, 0));
     // the VDIF invalid bit (word 0, bit 31) of each frame, for row flags
-    for (int64_t f = 0; f < nb; ++f)
-      s->finv[(size_t)((s->frames_in + f) % s->ring_frames)] = (src[f * pitch + 3] >> 7) & 1;
+    {
+      int64_t slot = s->frames_in % s->ring_frames;
+      for (int64_t f = 0; f < nb; ++f) {
+        s->finv[(size_t)slot] = (src[f * pitch + 3] >> 7) & 1;
+        if (++slot == s->ring_frames) slot = 0;
+      }
+    }
     // in-order pairs go straight to pair entries; the rest through the queue
     int64_t i = (int64_t)s->reader->run_fast(src, s->frames_in, (size_t)nb, s->e0, s->e1, pitch);
     for (; i < nb; ++i) {

@@ -154,33 +154,60 @@ size_t PairReader::run_fast(const uint8_t* fr, int64_t pay0, size_t n, std::vect
                             std::vector<int64_t>& e1, size_t pitch) {
   if (phase_ != RUNNING || !q_.empty() || nskip_[0] || nskip_[1]) return 0;
   const bool ts = mode_ == TS;
+  // Scan the pairs that continue the expected frame (and, TS, second)
+  // sequence; the state after the scan is that of the last pair, as the
+  // pair-by-pair path would leave it.
+  int x0 = expected_[0], x1 = expected_[1];
+  long long es0 = expsec_[0], es1 = expsec_[1];
+  int lf0 = 0, lf1 = 0;
+  long long ls0 = 0, ls1 = 0;
   size_t k = 0;
   for (; k + 1 < n; k += 2) {
-    uint32_t w0[2], w1[2];
-    for (int p = 0; p < 2; ++p) {
-      const uint8_t* h = fr + (k + p) * pitch;
-      std::memcpy(&w0[p], h, 4);  // seconds:30 | legacy | invalid (little-endian, vdifio.h:53-72)
-      std::memcpy(&w1[p], h + 4, 4);  // frame:24 | epoch:6 | unassigned:2
-    }
-    const int f0 = (int)(w1[0] & 0xFFFFFFu), f1 = (int)(w1[1] & 0xFFFFFFu);
-    if (f0 != expected_[0] || f1 != expected_[1]) break;  // a gap: checkframeskip decides
-    const long long s0 = w0[0] & 0x3FFFFFFFu, s1 = w0[1] & 0x3FFFFFFFu;
-    if (ts && (s0 != expsec_[0] || s1 != expsec_[1])) break;
+    const uint8_t* h0 = fr + k * pitch;
+    const uint8_t* h1 = h0 + pitch;
+    uint32_t a0, b0, a1, b1;
+    std::memcpy(&a0, h0, 4);  // seconds:30 | legacy | invalid (little-endian, vdifio.h:53-72)
+    std::memcpy(&b0, h0 + 4, 4);  // frame:24 | epoch:6 | unassigned:2
+    std::memcpy(&a1, h1, 4);
+    std::memcpy(&b1, h1 + 4, 4);
+    const int f0 = (int)(b0 & 0xFFFFFFu), f1 = (int)(b1 & 0xFFFFFFu);
+    if (f0 != x0 || f1 != x1) break;  // a gap: checkframeskip decides
+    const long long s0 = a0 & 0x3FFFFFFFu, s1 = a1 & 0x3FFFFFFFu;
+    if (ts && (s0 != es0 || s1 != es1)) break;
     // checkframeskip with no skip: advance the expected frame (and second)
-    expected_[0] = (f0 + 1) % kFramesPerSec;
-    expected_[1] = (f1 + 1) % kFramesPerSec;
+    x0 = f0 + 1 == kFramesPerSec ? 0 : f0 + 1;
+    x1 = f1 + 1 == kFramesPerSec ? 0 : f1 + 1;
     if (ts) {
-      expsec_[0] = s0 + (expected_[0] == 0 ? 1 : 0);
-      expsec_[1] = s1 + (expected_[1] == 0 ? 1 : 0);
+      es0 = s0 + (x0 == 0 ? 1 : 0);
+      es1 = s1 + (x1 == 0 ? 1 : 0);
     }
-    hdr_[0].frame = (uint32_t)f0;
-    hdr_[1].frame = (uint32_t)f1;
-    hdr_[0].seconds = (uint32_t)s0;
-    hdr_[1].seconds = (uint32_t)s1;
-    cur_[0] = pay0 + (int64_t)k;
-    cur_[1] = pay0 + (int64_t)k + 1;
-    e0.push_back(cur_[0]);
-    e1.push_back(cur_[1]);
+    lf0 = f0;
+    lf1 = f1;
+    ls0 = s0;
+    ls1 = s1;
+  }
+  if (k == 0) return 0;
+  expected_[0] = x0;
+  expected_[1] = x1;
+  if (ts) {
+    expsec_[0] = es0;
+    expsec_[1] = es1;
+  }
+  hdr_[0].frame = (uint32_t)lf0;
+  hdr_[1].frame = (uint32_t)lf1;
+  hdr_[0].seconds = (uint32_t)ls0;
+  hdr_[1].seconds = (uint32_t)ls1;
+  cur_[0] = pay0 + (int64_t)k - 2;
+  cur_[1] = pay0 + (int64_t)k - 1;
+  // pair j uses payloads pay0 + 2j (pol 0) and pay0 + 2j + 1 (pol 1)
+  const size_t np = k / 2, at = e0.size();
+  e0.resize(at + np);
+  e1.resize(at + np);
+  int64_t* o0 = e0.data() + at;
+  int64_t* o1 = e1.data() + at;
+  for (size_t j = 0; j < np; ++j) {
+    o0[j] = pay0 + 2 * (int64_t)j;
+    o1[j] = pay0 + 2 * (int64_t)j + 1;
   }
   return k;
 }
