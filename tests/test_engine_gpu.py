@@ -516,6 +516,49 @@ def test_stream_device_input_ordered_after_producer(vf):
             assert (x[key] is None and y[key] is None) or np.array_equal(x[key], y[key]), key
 
 
+def test_plans_on_host_threads_equal_sequential(vf):
+    """Several single-stream plans, each pushed and polled by its own host
+    thread at the same time (a plan is driven by one thread; plans are
+    independent), give per stream exactly the results of the same plans run
+    one after another: series, statistics and candidates bit-identical."""
+    import threading
+    dms = np.linspace(0.0, 40.0, 128).astype(np.float32)
+    bufs = [_vdif(3.0, seed=70 + i, pulses=[(1.0 + 0.2 * i, 10.0 + 8 * i, 2.0, 30.0)]) for i in range(4)]
+
+    def serve(i, out):
+        plan = vf.Plan(dms, nave=2, muoslowfreq=384.0, mode=vf.MODE_STREAM, chunk_seconds=0.25,
+                       outputs=vf.OUT_DEDISP | vf.OUT_DMSTATS | vf.OUT_CANDS, cand_snr=7.0)
+        rng = np.random.default_rng(i)
+        res, pos = [], 0
+        while pos < len(bufs[i]):
+            n = int(rng.integers(200000, 2000000))
+            plan.push(0, bufs[i][pos:pos + n])
+            pos += n
+            while (r := plan.poll(wait=False)) is not None:
+                res.append(r)
+        plan.push(0, None)
+        res += plan.drain()
+        plan.close()
+        out[i] = res
+
+    seq, par = {}, {}
+    for i in range(len(bufs)):
+        serve(i, seq)
+    threads = [threading.Thread(target=serve, args=(i, par)) for i in range(len(bufs))]
+    for t in threads:
+        t.start()
+    for t in threads:
+        t.join()
+    for i in range(len(bufs)):
+        a, b = seq[i], par[i]
+        assert len(a) == len(b) >= 4, i
+        for x, y in zip(a, b):
+            assert (x["seq"], x["row0"], x["nt"]) == (y["seq"], y["row0"], y["nt"])
+            for key in ("dd", "ave", "sigma", "peak", "frb", "argmax"):
+                assert np.array_equal(x[key], y[key]), (i, key)
+            assert x["cands"] == y["cands"] and y["device_errors"] == 0
+
+
 @pytest.mark.parametrize("storage", [0, 1])
 def test_stream_batched_dedispersion_equals_per_stream(vf, storage):
     """batch_streams = 1: the chunks that become ready in several streams are
