@@ -754,6 +754,8 @@ def main():
     # K1: compulsory bytes = raw VDIF read + FP32 filterbank written
     k1_ms = f32["stage_ms"][0]
     k1_bytes = data_s * (2 * 25600 * 5032 + nch * (1.0 / (NAVE * 12500 / 128e6)) * 4)
+    # K1 FFT work at the usual real-FFT count: 2.5 N log2 N per 12500-sample transform
+    k1_flop = data_s * 2 * (128e6 / 12500) * 2.5 * 12500 * math.log2(12500)
     roofline = {"bound": "fp32_add", "achieved": adds_per_s / 1e12, "peak": fp32_peak_adds / 1e12,
                 "unit": "Tadd/s", "frac": adds_per_s / fp32_peak_adds, "traffic": traffic,
                 "kernel": "dedisperse (K3)",
@@ -768,7 +770,14 @@ def main():
                 "k1_channelise": {"bound": "hbm", "achieved_gbs": k1_bytes / (k1_ms / 1000.0) / 1e9,
                                   "peak_gbs": hbm, "frac": k1_bytes / (k1_ms / 1000.0) / 1e9 / hbm,
                                   "bytes_per_step": k1_bytes,
-                                  "note": "compulsory bytes (raw VDIF in + FP32 filterbank out); peak " + peak_src}}
+                                  "note": "compulsory bytes (raw VDIF in + FP32 filterbank out); peak " + peak_src,
+                                  "fp32": {"achieved_tflops": k1_flop / (k1_ms / 1000.0) / 1e12,
+                                           "peak_tflops": 2 * fp32_peak_adds / 1e12,
+                                           "frac": k1_flop / (k1_ms / 1000.0) / (2 * fp32_peak_adds),
+                                           "flop_per_step": k1_flop,
+                                           "convention": "2.5 N log2 N flop per real N = 12500 transform, two "
+                                                         "per window (one per pol); peak = 2 flop x 128 FP32 "
+                                                         "lanes per SM x SMs x clock"}}}
     line = {
         "metric": METRIC,
         "value": rtf,
