@@ -132,6 +132,12 @@ typedef struct vfrb_bp_args {
   int32_t* d_err;
   int32_t subtract_mode;     /* 0: cal windows (subtractbpCAL); 1: copy only,
                               * no subtraction (feeds vfrb_subtract_bp_full)  */
+  void* out_shift1;          /* F16 only, or NULL (no reference counterpart):
+                              * device copy of `out` shifted by one row, same
+                              * strides and ring: absolute row R >= 1 of the
+                              * result also goes to row R - 1 here, so that
+                              * out_shift1[c][r] = out[c][r + 1]; pass it to
+                              * vfrb_dedisperse as fb_shift1               */
 } vfrb_bp_args;
 int vfrb_bandpass(const vfrb_bp_args* a, void* stream);
 
@@ -215,6 +221,13 @@ typedef struct vfrb_dd_args {
   int32_t* frb;
   int32_t* argmax;
   int32_t* d_err;
+  const void* fb_shift1;     /* F16 only, or NULL (no reference counterpart):
+                              * `fb` shifted by one row (fb_shift1[c][r] =
+                              * fb[c][r + 1] for every row but the last valid
+                              * one; vfrb_bp_args.out_shift1 writes it).  The
+                              * four-trial pattern kernel then reads windows of
+                              * halves with 4-byte loads; results equal the
+                              * plain FP16 form's up to FP32 summation order */
 } vfrb_dd_args;
 size_t vfrb_dedisperse_workspace_bytes(const vfrb_ddplan* plan, int64_t nt_out);
 int vfrb_dedisperse(const vfrb_ddplan* plan, const vfrb_dd_args* a, void* stream);

@@ -441,6 +441,84 @@ def test_dedisperse_ring_wrap(vf, O):
         assert np.max(np.abs(out.cpu().numpy() - ref)) <= 1e-5 * np.sqrt(np.mean(ref ** 2)), v
 
 
+def test_bandpass_fp16_shifted_copy(vf, O):
+    """FP16 bandpass with out_shift1: the second ring holds the result shifted
+    by one row (row R - 1 of it = row R of the result, absolute rows, ring
+    wrap included), bit for bit; rows it does not cover keep their contents."""
+    torch = _torch()
+    rows, nch = 384, 48
+    x = _rand_fb(rows, nch, seed=12)
+    dev = torch.device("cuda")
+    inv = torch.full((nch,), 0.25, device=dev)
+    for out_row0, mask in ((0, 0xFFFFFFFF), (1000, 1023)):
+        R = 2048 if mask == 0xFFFFFFFF else mask + 1
+        out = torch.zeros((nch, R), dtype=torch.float16, device=dev)
+        out1 = torch.full((nch, R), 7.0, dtype=torch.float16, device=dev)
+        vf.bandpass(torch.from_numpy(x).to(dev), storage=vf.F16, out=out, out_row0=out_row0, out_row_mask=mask,
+                    inv_scale=inv, out_shift1=out1)
+        torch.cuda.synchronize()
+        a, b = out.cpu().numpy(), out1.cpu().numpy()
+        rr = (out_row0 + np.arange(rows)) & (R - 1)
+        sh = (out_row0 - 1 + np.arange(rows)) & (R - 1)
+        ok = out_row0 - 1 + np.arange(rows) >= 0
+        assert np.array_equal(b[:, sh[ok]].view(np.uint16), a[:, rr[ok]].view(np.uint16))
+        untouched = np.setdiff1d(np.arange(R), sh[ok])
+        assert np.all(b[:, untouched] == 7.0)
+
+
+@pytest.mark.parametrize("irregular", [False, True])
+@pytest.mark.parametrize("wrap", [False, True])
+def test_dedisperse_fp16_pair_form(vf, O, irregular, wrap):
+    """FP16 four-trial pattern kernel given the ring shifted by one row
+    (fb_shift1): windows of halves read with 4-byte loads from the copy that
+    aligns them.  The series equal the plain FP16 form's (same FP16 values,
+    FP32 sums in another channel order: <= 2e-6 of the rms) and the FP64
+    oracle's (<= 1e-5 of the rms), statistics match, and rows the kernel must
+    not use -- outside the valid rows of the ring, and the shifted copy's row
+    that would hold the first invalid row -- are NaN without reaching the
+    output.  The irregular DM list drives the generic (per-trial) path."""
+    torch = _torch()
+    dms, off, md, fb = _dd_case(ndm=70, nch=320, nt=1500, seed=21, dm_max=8.0, irregular=irregular)
+    nt = 1500
+    plan = vf.DedispPlan(off)
+    assert plan.group_size == 4
+    rows = fb.shape[0]
+    R = 1 << int(np.ceil(np.log2(rows + 64)))
+    r0 = R - 300 if wrap else 16
+    nanh = np.float16("nan")
+    ring = np.full((fb.shape[1], R), nanh, np.float16)
+    ridx = (r0 + np.arange(rows)) & (R - 1)
+    ring[:, ridx] = fb.T.astype(np.float16)
+    ring1 = np.full_like(ring, nanh)
+    # shifted copy of FB rows r0 .. r0 + rows - 1: its rows r0 - 1 .. r0 + rows - 2; its row
+    # r0 + rows - 1 (the first invalid FB row) stays NaN
+    ring1[:, (r0 - 1 + np.arange(rows)) & (R - 1)] = ring[:, (r0 + np.arange(rows)) & (R - 1)]
+    ref = O.dedisperse(fb.astype(np.float16).astype(np.float64), off, nt) * 0.5
+    st_ref = O.calcstats_dm(ref)
+    rms = np.sqrt(np.mean(ref ** 2))
+    dev = torch.device("cuda")
+    x, x1 = torch.from_numpy(ring).to(dev), torch.from_numpy(ring1).to(dev)
+    plan.set_variant(vf.F16, vf.DD_PAT4)
+    res = []
+    for shifted in (None, x1):
+        err = torch.zeros(1, dtype=torch.int32, device=dev)
+        out, st = plan(x, nt, storage=vf.F16, uniform_scale=0.5, row0=r0, row_mask=R - 1, nrows_valid=rows,
+                       d_err=err, fb_shift1=shifted)
+        torch.cuda.synchronize()
+        assert int(err.item()) == 0
+        got = out.cpu().numpy()
+        assert np.all(np.isfinite(got))
+        e = np.max(np.abs(got - ref)) / rms
+        print(f"pair={shifted is not None} irregular={irregular} wrap={wrap}: err/rms {e:.2e}")
+        assert e <= 1e-5
+        assert np.array_equal(st["frb"].cpu().numpy(), st_ref["frb"])
+        assert np.allclose(st["peak"].cpu().numpy(), st_ref["peak"], rtol=1e-4)
+        res.append(got)
+    d = np.max(np.abs(res[0] - res[1])) / rms
+    print("pair vs plain FP16 form: max diff / rms", d)
+    assert d <= 2e-6
+
+
 def test_dedisperse_sigma_matches_fp64(vf, O):
     """dedisperseSTATS (TS:1450-1481)."""
     torch = _torch()

@@ -72,7 +72,8 @@ class BpArgs(C.Structure):
                 ("storage", C.c_int32), ("out", C.c_void_p), ("out_chan_stride", C.c_int64),
                 ("out_row0", C.c_int64), ("out_row_mask", C.c_uint32), ("inv_scale", C.c_void_p),
                 ("q_scale", C.c_float), ("win_mean", C.c_void_p), ("win_var", C.c_void_p), ("tm_out", C.c_void_p),
-                ("tm_row_stride", C.c_int64), ("d_err", C.c_void_p), ("subtract_mode", C.c_int32)]
+                ("tm_row_stride", C.c_int64), ("d_err", C.c_void_p), ("subtract_mode", C.c_int32),
+                ("out_shift1", C.c_void_p)]
 
 
 class DdArgs(C.Structure):
@@ -81,7 +82,7 @@ class DdArgs(C.Structure):
                 ("nrows_valid", C.c_int64), ("nt_out", C.c_int64), ("out", C.c_void_p), ("out_stride", C.c_int64),
                 ("sigma_out", C.c_void_p), ("workspace", C.c_void_p), ("workspace_bytes", C.c_size_t),
                 ("ave", C.c_void_p), ("sigma", C.c_void_p), ("peak", C.c_void_p), ("frb", C.c_void_p),
-                ("argmax", C.c_void_p), ("d_err", C.c_void_p)]
+                ("argmax", C.c_void_p), ("d_err", C.c_void_p), ("fb_shift1", C.c_void_p)]
 
 
 class CsArgs(C.Structure):
@@ -191,7 +192,7 @@ def channelise(frames, slots0, slots1, sample0: int, nrows: int, L: Layout, out=
 
 def bandpass(fb_tm, nrows=None, storage=F32, out=None, out_row0=0, out_row_mask=0xFFFFFFFF, inv_scale=None,
              q_scale=16.0, in_row0=0, in_row_mask=0xFFFFFFFF, window=128, win_mean=None, win_var=None,
-             tm_out=None, d_err=None, subtract_mode=0, stream=None):
+             tm_out=None, d_err=None, subtract_mode=0, out_shift1=None, stream=None):
     torch = _torch()
     nrows = fb_tm.shape[0] if nrows is None else nrows
     nchan = fb_tm.shape[1]
@@ -203,7 +204,7 @@ def bandpass(fb_tm, nrows=None, storage=F32, out=None, out_row0=0, out_row_mask=
                out_chan_stride=out.stride(0), out_row0=out_row0, out_row_mask=out_row_mask,
                inv_scale=_ptr(inv_scale), q_scale=q_scale, win_mean=_ptr(win_mean), win_var=_ptr(win_var),
                tm_out=_ptr(tm_out), tm_row_stride=tm_out.stride(0) if tm_out is not None else 0,
-               d_err=_ptr(d_err), subtract_mode=subtract_mode)
+               d_err=_ptr(d_err), subtract_mode=subtract_mode, out_shift1=_ptr(out_shift1))
     _check(_lib.vfrb_bandpass(C.byref(a), _stream(stream)), "vfrb_bandpass")
     return out
 
@@ -267,7 +268,8 @@ class DedispPlan:
         return int(_lib.vfrb_dedisperse_workspace_bytes(self._p, nt_out))
 
     def __call__(self, fb_cm, nt_out: int, storage=F32, chan_scale=None, uniform_scale=0.0, row0=0, row_mask=0xFFFFFFFF,
-                 nrows_valid=None, out=None, sigma_out=None, stats=True, workspace=None, d_err=None, stream=None):
+                 nrows_valid=None, out=None, sigma_out=None, stats=True, workspace=None, d_err=None, fb_shift1=None,
+                 stream=None):
         torch = _torch()
         dev = fb_cm.device
         if out is None:
@@ -288,7 +290,8 @@ class DedispPlan:
                    out=out.data_ptr(), out_stride=out.stride(0), sigma_out=_ptr(sigma_out),
                    workspace=_ptr(workspace), workspace_bytes=workspace.numel() if workspace is not None else 0,
                    ave=_ptr(st.get("ave")), sigma=_ptr(st.get("sigma")), peak=_ptr(st.get("peak")),
-                   frb=_ptr(st.get("frb")), argmax=_ptr(st.get("argmax")), d_err=_ptr(d_err))
+                   frb=_ptr(st.get("frb")), argmax=_ptr(st.get("argmax")), d_err=_ptr(d_err),
+                   fb_shift1=_ptr(fb_shift1))
         _check(_lib.vfrb_dedisperse(self._p, C.byref(a), _stream(stream)), "vfrb_dedisperse")
         return out, st
 

@@ -10,7 +10,10 @@
 // (512-byte runs per channel), the layout the dedisperser streams, in FP32,
 // FP16 (z = x/s_c) or int8 (round(z*q)) form.  subtract_mode 1 skips the
 // statistics and writes the rows unchanged (the input of the whole-block
-// subtractbp in rfi.cu).
+// subtractbp in rfi.cu).  The FP16 form can also write a copy shifted by one
+// row, out1[c][r - 1] = out[c][r] (absolute rows, the same ring geometry):
+// with both copies the dedisperser reads any window of halves with aligned
+// 4-byte loads.
 #include "vfrb_common.cuh"
 
 namespace vfrb {
@@ -31,7 +34,7 @@ __device__ __forceinline__ int warp_sum_i(int v) {
 }
 
 template <int STORAGE>
-__global__ void __launch_bounds__(kBpThreads) k_bandpass(const vfrb_bp_args a) {
+__global__ void __launch_bounds__(kBpThreads) k_bandpass(const vfrb_bp_args a, __half* __restrict__ out1) {
   __shared__ float tile[kBpChan][kBpMaxWin + 1];
   const int win = blockIdx.y;
   const int c0 = blockIdx.x * kBpChan;
@@ -109,7 +112,12 @@ __global__ void __launch_bounds__(kBpThreads) k_bandpass(const vfrb_bp_args a) {
         if (STORAGE == VFRB_F32) {
           reinterpret_cast<float*>(a.out)[o] = y;
         } else if (STORAGE == VFRB_F16) {
-          reinterpret_cast<__half*>(a.out)[o] = __float2half_rn(y * inv);
+          const __half h = __float2half_rn(y * inv);
+          reinterpret_cast<__half*>(a.out)[o] = h;
+          const long long ra = a.out_row0 + r0 + r;  // absolute row; row ra - 1 of the shifted copy
+          if (out1 && ra >= 1)
+            out1[(long long)c * a.out_chan_stride +
+                 (long long)((unsigned long long)(ra - 1) & (unsigned long long)a.out_row_mask)] = h;
         } else {
           float q = rintf(y * inv * a.q_scale);
           q = fminf(fmaxf(q, -127.f), 127.f);
@@ -131,15 +139,16 @@ __global__ void __launch_bounds__(kBpThreads) k_bandpass(const vfrb_bp_args a) {
 
 int launch_bandpass(const vfrb_bp_args& a, cudaStream_t s) {
   if (a.nrows <= 0) return a.nrows == 0 ? VFRB_OK : VFRB_ERR_ARG;
+  if (a.out_shift1 && (a.storage != VFRB_F16 || a.out_row0 < 0 || ((uintptr_t)a.out_shift1 & 1))) return VFRB_ERR_ARG;
   if (!a.in || !a.out || a.nchan <= 0 || a.window <= 0 || a.window > kBpMaxWin) return VFRB_ERR_ARG;
   if (a.storage != VFRB_F32 && !a.inv_scale) return VFRB_ERR_ARG;
   if (a.subtract_mode != 0 && a.subtract_mode != 1) return VFRB_ERR_ARG;
   const int nwin = (a.nrows + a.window - 1) / a.window;
   dim3 grid((a.nchan + kBpChan - 1) / kBpChan, nwin);
   switch (a.storage) {
-    case VFRB_F32: k_bandpass<VFRB_F32><<<grid, kBpThreads, 0, s>>>(a); break;
-    case VFRB_F16: k_bandpass<VFRB_F16><<<grid, kBpThreads, 0, s>>>(a); break;
-    case VFRB_I8: k_bandpass<VFRB_I8><<<grid, kBpThreads, 0, s>>>(a); break;
+    case VFRB_F32: k_bandpass<VFRB_F32><<<grid, kBpThreads, 0, s>>>(a, nullptr); break;
+    case VFRB_F16: k_bandpass<VFRB_F16><<<grid, kBpThreads, 0, s>>>(a, static_cast<__half*>(a.out_shift1)); break;
+    case VFRB_I8: k_bandpass<VFRB_I8><<<grid, kBpThreads, 0, s>>>(a, nullptr); break;
     default: return VFRB_ERR_ARG;
   }
   return cuda_status(cudaGetLastError());

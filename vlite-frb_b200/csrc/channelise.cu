@@ -55,21 +55,22 @@ constexpr int kStage = 12512;          // one pol's window bytes, padded to 16
 constexpr int kStageT0 = 64;
 constexpr int kStageThreads = kPThreads - kStageT0;
 
-// Twiddle tables, as (c, c, s, s) so a twiddle is one packed pair per
-// component, computed on the host in double precision:
-//   g_pw2[(r-1)*25 + m] = W_625^(m r)   (pass 2, Ns = 25)
-//   g_pw12[j] = W_12500^j, j < 625       (the real-split twiddle of pass 3;
-//                                         its square W_6250^j seeds pass 3's
-//                                         own twiddles)
+// Twiddle tables, computed on the host in double precision:
+//   g_pw2[(r-1)*25 + m] = W_625^(m r) as (c, c, s, s), so a twiddle is one
+//                         packed pair per component   (pass 2, Ns = 25)
+//   g_pw12[m] = W_12500^m as (c, s), m < 6250: pass 3 reads its real-split
+//                         twiddles W_12500^(j + 625 k) and its radix-10 seed
+//                         W_6250^j = W_12500^(2 j) here instead of building
+//                         them by repeated complex products
 constexpr int kPTw2 = 24 * 25;
-constexpr int kPT12 = 625;
+constexpr int kPT12 = kH;
 __device__ float4 g_pw2[kPTw2];
-__device__ float4 g_pw12[kPT12];
+__device__ float2 g_pw12[kPT12];
 
-// shared memory: Z | tw2 | t12 | codelet constants + W_20 | staged bytes
+// shared memory: Z | tw2 | codelet constants | t12 | staged bytes
 // [2 buffers][2 pols][kStage]
 constexpr size_t kPSmZ = sizeof(float4) * kH;
-constexpr size_t kPSmTab = sizeof(float4) * (kPTw2 + kPT12 + kPairTable + 1);
+constexpr size_t kPSmTab = sizeof(float4) * (kPTw2 + kPairTable) + sizeof(float2) * kPT12;
 constexpr size_t kPSmem = kPSmZ + kPSmTab + 4 * kStage;
 static_assert(kPSmem <= 227 * 1024, "channeliser shared memory");
 static_assert(kPB <= kPThreads && kPTasks <= 2 * kPThreads, "pass-3 tasks in two rounds");
@@ -83,14 +84,18 @@ static int ensure_twiddles() {
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return VFRB_ERR_CUDA;
   std::lock_guard<std::mutex> lk(g_tw_mu);
   if (g_tw_ready[dev]) return VFRB_OK;
-  static float4 p2[kPTw2], p12[kPT12];
+  static float4 p2[kPTw2];
+  static float2 p12[kPT12];
   auto quad = [](double num, double den) {
     const double a = -2.0 * M_PI * num / den;
     return make_float4((float)cos(a), (float)cos(a), (float)sin(a), (float)sin(a));
   };
   for (int r = 1; r < 25; ++r)
     for (int m = 0; m < 25; ++m) p2[(r - 1) * 25 + m] = quad((double)((m * r) % 625), 625.0);
-  for (int j = 0; j < kPT12; ++j) p12[j] = quad((double)j, 12500.0);
+  for (int j = 0; j < kPT12; ++j) {
+    const double a = -2.0 * M_PI * (double)j / 12500.0;
+    p12[j] = make_float2((float)cos(a), (float)sin(a));
+  }
   if (cudaMemcpyToSymbol(g_pw2, p2, sizeof(p2)) != cudaSuccess) return VFRB_ERR_CUDA;
   if (cudaMemcpyToSymbol(g_pw12, p12, sizeof(p12)) != cudaSuccess) return VFRB_ERR_CUDA;
   g_tw_ready[dev] = true;
@@ -110,6 +115,9 @@ struct Rot {
 };
 __device__ __forceinline__ Rot rot_of(float4 q) {
   return Rot{make_float2(q.x, q.y), make_float2(q.z, q.w), make_float2(-q.z, -q.w)};
+}
+__device__ __forceinline__ Rot rot_of2(float2 q) {
+  return Rot{make_float2(q.x, q.x), make_float2(q.y, q.y), make_float2(-q.y, -q.y)};
 }
 __device__ __forceinline__ Rot rot_mul(const Rot& a, const Rot& b) {
   return Rot{f2fma(a.s, b.ns, f2mul(a.c, b.c)), f2fma(a.s, b.c, f2mul(a.c, b.s)), f2fma(a.ns, b.c, f2mul(a.c, b.ns))};
@@ -222,19 +230,17 @@ __device__ __forceinline__ void pp_emit(float* dst, int bin, int nskip, int ncha
 }
 
 // Pass 3 (radix 10, Ns = 625) of butterfly j and its mirror 625 - j, the
-// real split and detection.  j = 0 is its own mirror.  kt[kPairTable] holds
-// W_20 = W_12500^625, the step between the bins of one butterfly.
-__device__ __forceinline__ void pp_pass3(const float4* __restrict__ Z, const float4* __restrict__ t12,
+// real split and detection.  j = 0 is its own mirror.  t12[m] = W_12500^m.
+__device__ __forceinline__ void pp_pass3(const float4* __restrict__ Z, const float2* __restrict__ t12,
                                          const float4* __restrict__ kt, int j, float* dst, int nskip, int nchanout,
                                          bool first, float scale) {
   PolPair u[10], d[10];
-  const Rot q = rot_of(t12[j]);  // W_12500^j
   if (j == 0) {
 #pragma unroll
     for (int r = 0; r < 10; ++r) u[r] = pp_unpack(Z[kPM3 * r]);
     dft10p(u, kt);
   } else {
-    const Rot w1 = rot_mul(q, q);  // W_6250^j
+    const Rot w1 = rot_of2(t12[2 * j]);  // W_6250^j
     Rot wr = w1;
     u[0] = pp_unpack(Z[j]);
     d[0] = pp_unpack(Z[kPM3 - j]);
@@ -251,11 +257,11 @@ __device__ __forceinline__ void pp_pass3(const float4* __restrict__ Z, const flo
     dft10p(u, kt);
     dft10p(d, kt);
   }
-  Rot wk = q;  // W_12500^(j + 625 k)
   const int kend = j == 0 ? 6 : 10;
 #pragma unroll
   for (int k = 0; k < 10; ++k) {
     if (k < kend) {
+      const Rot wk = rot_of2(t12[j + kPM3 * k]);  // W_12500^(j + 625 k), j + 625 k < 6250
       // Z[k'] with k' = j + 625 k, and Z[H - k'] (butterfly 625 - j, output
       // 9 - k, which its twiddle shift leaves at index 10 - k)
       const PolPair zk = u[dft10p_pos(k)];
@@ -272,7 +278,6 @@ __device__ __forceinline__ void pp_pass3(const float4* __restrict__ Z, const flo
       const int bin = j + kPM3 * k;
       pp_emit(dst, bin, nskip, nchanout, first, (pu.x + pu.y) * scale);
       if (bin != kH - bin) pp_emit(dst, kH - bin, nskip, nchanout, first, (pv.x + pv.y) * scale);
-      if (k < 9) wk = rot_mul(wk, rot_of(kt[kPairTable]));
     }
   }
 }
@@ -282,16 +287,14 @@ __global__ void __launch_bounds__(kPThreads, 1) k_channelise(const vfrb_chan_arg
   extern __shared__ float4 smem_f4[];
   float4* Z = smem_f4;
   float4* tw2 = smem_f4 + kH;
-  float4* t12 = tw2 + kPTw2;
-  float4* ktab = t12 + kPT12;  // codelet constants, then W_20 (pass 3's bin step)
-  unsigned char* stage = reinterpret_cast<unsigned char*>(ktab + kPairTable + 1);  // [2 buffers][2 pols][kStage]
+  float4* ktab = tw2 + kPTw2;  // codelet constants
+  float2* t12 = reinterpret_cast<float2*>(ktab + kPairTable);
+  unsigned char* stage = reinterpret_cast<unsigned char*>(t12 + kPT12);  // [2 buffers][2 pols][kStage]
   const int tid = threadIdx.x;
   int err = 0;
   for (int i = tid; i < kPTw2; i += kPThreads) tw2[i] = g_pw2[i];
   for (int i = tid; i < kPT12; i += kPThreads) t12[i] = g_pw12[i];
   if (tid < kPairTable) ktab[tid] = c_pair_table[tid];
-  if (tid == kPairTable)
-    ktab[tid] = make_float4(9.510565163e-01f, 9.510565163e-01f, -3.090169944e-01f, -3.090169944e-01f);
   // the staging buffers' padding (never written by the copies) holds the
   // zero read below: 3 ints in each of the 4 pol buffers
   if (tid < 4 * ((kStage - kFftN) / 4)) {
@@ -329,7 +332,7 @@ __global__ void __launch_bounds__(kPThreads, 1) k_channelise(const vfrb_chan_arg
     const int z = *reinterpret_cast<const volatile int*>(cur + kFftN);
     const float4* kt = ktab + z;
     const float4* tw = tw2 + z;
-    const float4* tj = t12 + z;
+    const float2* tj = t12 + z;
     if (tid < kPB) {  // pass 1: R = 25, Ns = 1, from the staged bytes
       PolPair v[25];
 #pragma unroll

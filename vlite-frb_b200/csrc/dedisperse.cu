@@ -549,10 +549,12 @@ static int reg_launch(const vfrb_ddplan* pl, int v, const vfrb_dd_args& a, DmPar
   return VFRB_OK;
 }
 
-template <typename T, int D, int TT, int SMAX, int W>
+template <typename T, int D, int TT, int SMAX, int W, bool PAIR = false>
 static int pat_launch_t(const vfrb_ddplan* pl, const RegGroup& g, const vfrb_dd_args& a, DmPartial* part,
-                        float out_scale, cudaStream_t s, int* ntb, const DdJob* jobs = nullptr, int njobs = 0) {
+                        float out_scale, cudaStream_t s, int* ntb, const DdJob* jobs = nullptr, int njobs = 0,
+                        const void* fb1 = nullptr) {
   constexpr int VEC = 16 / (int)sizeof(T);
+  constexpr int NCOPY = PAIR ? 2 : 1;
   constexpr int NT = 32 * TT;
   *ntb = 0;
   if (g.D != D || g.smax > SMAX || !g.d_gpat) return VFRB_OK;  // not applicable
@@ -566,11 +568,12 @@ static int pat_launch_t(const vfrb_ddplan* pl, const RegGroup& g, const vfrb_dd_
   // 8 warps: two CTAs per SM, each under ~110 KB of shared memory; 16 warps:
   // one CTA per SM with ~220 KB
   const int budget = (W == 16 ? 220 : 110) * 1024;
-  const int per_ch = 2 * lm * (int)sizeof(T) + 3 * W * 4;
+  const int per_ch = 2 * NCOPY * lm * (int)sizeof(T) + 3 * W * 4;
   const int chunk = std::min(32, (budget - W * 4 - 32) / per_ch);
   if (chunk < 4) return VFRB_OK;
   DdPatParams k{};
   k.fb = a.fb;
+  k.fb1 = fb1;
   k.out_scale = out_scale;
   k.chan_stride = a.chan_stride;
   k.row0 = a.row0;
@@ -593,9 +596,9 @@ static int pat_launch_t(const vfrb_ddplan* pl, const RegGroup& g, const vfrb_dd_
   k.njobs = njobs;
   for (int i = 0; i < njobs; ++i) k.jobs[i] = jobs[i];
   const size_t meta = 16 + ((size_t)3 * W * chunk + W + 3) / 4 * 16;
-  const size_t smem = meta + (size_t)2 * chunk * lm * sizeof(T);
-  cudaError_t e =
-      cudaFuncSetAttribute(k_dedisp_pat<T, D, TT, SMAX, W>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  const size_t smem = meta + (size_t)2 * NCOPY * chunk * lm * sizeof(T);
+  cudaError_t e = cudaFuncSetAttribute(k_dedisp_pat<T, D, TT, SMAX, W, PAIR>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return VFRB_ERR_CUDA;
   const long long ntime = (a.nt_out + NT - 1) / NT;
   // grid y runs time blocks shifted by each DM block's delay at the middle
@@ -603,15 +606,16 @@ static int pat_launch_t(const vfrb_ddplan* pl, const RegGroup& g, const vfrb_dd_
   const long long ny = ntime + mid_max / NT;
   if (ny > 65535) return VFRB_OK;
   dim3 grid((unsigned)nblocks, (unsigned)ny, (unsigned)std::max(1, njobs));
-  k_dedisp_pat<T, D, TT, SMAX, W><<<grid, W * 32, smem, s>>>(k);
+  k_dedisp_pat<T, D, TT, SMAX, W, PAIR><<<grid, W * 32, smem, s>>>(k);
   const int st = cuda_status(cudaGetLastError());
   if (st == VFRB_OK) *ntb = (int)ntime;
   return st;
 }
 
 // Pattern-run variant `v` for this call; *ntb == 0 when it does not apply.
+// fb1 (FP16 only, or NULL): the ring shifted by one row, for the pair form.
 static int pat_launch(const vfrb_ddplan* pl, int v, const vfrb_dd_args& a, DmPartial* part, cudaStream_t s,
-                      int* ntb, const DdJob* jobs = nullptr, int njobs = 0) {
+                      int* ntb, const DdJob* jobs = nullptr, int njobs = 0, const void* fb1 = nullptr) {
   *ntb = 0;
   if (((uintptr_t)a.fb & 15) != 0) return VFRB_OK;
   const int D = v == VFRB_DD_PAT4 ? 4 : 2;
@@ -629,6 +633,13 @@ static int pat_launch(const vfrb_ddplan* pl, int v, const vfrb_dd_args& a, DmPar
   if (a.storage == VFRB_F16) {
     if (a.chan_scale || !(a.uniform_scale > 0.f)) return VFRB_OK;
     if (a.chan_stride % 8 || ((unsigned long long)a.row_mask + 1ULL) % 8) return VFRB_OK;
+    // with the shifted copy: the pair form (two staged copies per row, so the
+    // 16-warp CTA's tiles are the FP32 form's size)
+    if (D == 4 && fb1 && ((uintptr_t)fb1 & 15) == 0) {
+      const int st = pat_launch_t<__half, 4, 14, VFRB_PAT4_SMAX, 16, true>(pl, *g, a, part, a.uniform_scale, s, ntb,
+                                                                          jobs, njobs, fb1);
+      if (st || *ntb) return st;  // else (tiles too large for the pair form) the plain FP16 form below
+    }
     if (D == 4)
       return pat_launch_t<__half, 4, 14, VFRB_PAT4_SMAX, 8>(pl, *g, a, part, a.uniform_scale, s, ntb, jobs, njobs);
     return pat_launch_t<__half, 2, 26, VFRB_PAT2_SMAX, 8>(pl, *g, a, part, a.uniform_scale, s, ntb, jobs, njobs);
@@ -655,7 +666,8 @@ static int default_variant(const vfrb_ddplan* pl, int storage) {
   return VFRB_DD_STAGED;
 }
 
-static int launch_variant(const vfrb_ddplan* pl, int v, const vfrb_dd_args& a, cudaStream_t s) {
+static int launch_variant(const vfrb_ddplan* pl, int v, const vfrb_dd_args& a, cudaStream_t s,
+                          const void* fb1 = nullptr) {
   const bool want_stats = a.ave || a.sigma || a.peak || a.frb || a.argmax;
   DdKParams k{};
   k.fb = a.fb;
@@ -677,7 +689,8 @@ static int launch_variant(const vfrb_ddplan* pl, int v, const vfrb_dd_args& a, c
   int ntb = 0, st = VFRB_OK;
   if (!a.sigma_out && (v == VFRB_DD_REG1 || v == VFRB_DD_REG2 || v == VFRB_DD_REG4))
     st = reg_launch(pl, v, a, k.part, s, &ntb);
-  if (!a.sigma_out && (v == VFRB_DD_PAT4 || v == VFRB_DD_PAT2)) st = pat_launch(pl, v, a, k.part, s, &ntb);
+  if (!a.sigma_out && (v == VFRB_DD_PAT4 || v == VFRB_DD_PAT2))
+    st = pat_launch(pl, v, a, k.part, s, &ntb, nullptr, 0, a.storage == VFRB_F16 ? fb1 : nullptr);
   if (st) return st;
   if (ntb == 0) {
     const bool staged = v != VFRB_DD_DIRECT;
@@ -716,7 +729,7 @@ int launch_dedisperse_plan(const vfrb_ddplan* pl, const vfrb_dd_args& a, cudaStr
     return VFRB_ERR_ARG;
   int v = pl->variant[a.storage];
   if (v == VFRB_DD_AUTO) v = default_variant(pl, a.storage);
-  return launch_variant(pl, v, a, s);
+  return launch_variant(pl, v, a, s, a.fb_shift1);
 }
 
 // One launch of the pattern kernel over several streams' chunks (grid z =
@@ -741,7 +754,9 @@ int launch_dedisperse_jobs(const vfrb_ddplan* pl, int storage, const DdJob* jobs
   a.row_mask = row_mask;
   a.nrows_valid = jobs[0].nrows_valid;
   long long nt = 0;
+  bool pair = storage == VFRB_F16;  // every job has its shifted copy
   for (int i = 0; i < njobs; ++i) {
+    pair = pair && jobs[i].fb1 != nullptr;
     nt = std::max(nt, jobs[i].nt_out);
     if (((uintptr_t)jobs[i].fb & 15) != 0 || (storage == VFRB_F16 && !(jobs[i].out_scale > 0.f)) ||
         jobs[i].nrows_valid < jobs[i].nt_out + pl->max_delay)
@@ -751,7 +766,7 @@ int launch_dedisperse_jobs(const vfrb_ddplan* pl, int storage, const DdJob* jobs
   a.out = jobs[0].out;
   a.out_stride = jobs[0].out_stride;
   int ntb = 0;
-  const int st = pat_launch(pl, v, a, nullptr, s, &ntb, jobs, njobs);
+  const int st = pat_launch(pl, v, a, nullptr, s, &ntb, jobs, njobs, pair ? jobs[0].fb1 : nullptr);
   if (st) return st;
   *launched = ntb > 0;
   return VFRB_OK;

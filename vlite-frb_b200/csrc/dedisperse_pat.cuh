@@ -20,6 +20,16 @@
 // Lanes own TT-sample runs with TT odd (FP32) or TT = 2 mod 4 (FP16), so the
 // 32 lanes of a load touch 32 different banks.  Groups whose pattern is not
 // in the table take a generic path (one dispatch per trial and channel).
+//
+// FP16 pair form (PAIR): the bandpass also writes the FP16 ring shifted by
+// one row (fb1[c][r] = fb[c][r + 1]), and each staged channel row is copied
+// from both rings.  With TT even, a window's start parity is the channel's
+// (warp-uniform), so the window is read from the copy that puts its start on
+// a 4-byte boundary: one 32-bit load per two halves, which halves both the
+// shared-load instructions and the shared-memory wavefronts of the 2-byte
+// loads (a warp's 2-byte load moves 64 bytes, its 4-byte load 128).  The
+// adds, their order and the FP32 accumulation are those of the plain FP16
+// form.
 #pragma once
 
 #include "dedisp_patterns.cuh"
@@ -34,6 +44,7 @@ struct DdPatParams {
   int njobs;                   // 0: one launch with the fields below; else jobs[blockIdx.z] overrides them
   DdJob jobs[kDdMaxJobs];
   const void* fb;
+  const void* fb1;             // PAIR form: fb shifted by one row
   float out_scale;  // multiplies sum/nchan (1 for FP32, S for FP16)
   long long chan_stride;
   long long row0;
@@ -121,6 +132,73 @@ __device__ __forceinline__ void pat_run(float (&acc)[D][TT], const T* tile, cons
   }
 }
 
+// PAIR form: window element m is half (m & 1) of word w[m >> 1]; a
+// register split (mov.b32 {lo, hi}) rather than shifts, so the halves can
+// feed the mixed-precision adds directly
+template <int NW2>
+__device__ __forceinline__ void split_halves(const unsigned (&w)[NW2], unsigned short (&h)[2 * NW2]) {
+#pragma unroll
+  for (int k = 0; k < NW2; ++k) asm("mov.b32 {%0, %1}, %2;" : "=h"(h[2 * k]), "=h"(h[2 * k + 1]) : "r"(w[k]));
+}
+template <int D, int TT, int NH, int J, int S0, int... SR>
+__device__ __forceinline__ void pat_add_pair(float (&acc)[D][TT], const unsigned short (&h)[NH]) {
+#pragma unroll
+  for (int t = 0; t < TT; ++t) acc[J][t] = add_h(acc[J][t], h[t + S0]);
+  if constexpr (sizeof...(SR) > 0) pat_add_pair<D, TT, NH, J + 1, SR...>(acc, h);
+}
+// n channels of one run, PAIR form: slot entries are even element offsets
+// into the copy that aligns the window
+template <int D, int TT, int... S>
+__device__ __forceinline__ void pat_run_pair(float (&acc)[D][TT], const __half* tile, const int* slot, int n,
+                                             int lane_off) {
+  constexpr int NW2 = (TT + PatMax<S...>::v + 1) / 2;
+  int sl = slot[0];
+#pragma unroll 1
+  for (int i = 0; i < n; ++i) {
+    const unsigned* src = reinterpret_cast<const unsigned*>(tile + sl + lane_off);
+    sl = slot[i + 1];
+    unsigned w[NW2];
+#pragma unroll
+    for (int k = 0; k < NW2; ++k) w[k] = src[k];
+    unsigned short h[2 * NW2];
+    split_halves<NW2>(w, h);
+    pat_add_pair<D, TT, 2 * NW2, 0, S...>(acc, h);
+  }
+}
+template <int TT, int NH, int S>
+__device__ __forceinline__ void pat_add_one_pair(float (&acc)[TT], const unsigned short (&h)[NH]) {
+#pragma unroll
+  for (int t = 0; t < TT; ++t) acc[t] = add_h(acc[t], h[t + S]);
+}
+template <int D, int TT, int SMAX>
+__device__ __forceinline__ void pat_run_generic_pair(float (&acc)[D][TT], const __half* tile, const int* slot,
+                                                     const unsigned* pk, int n, int lane_off) {
+  constexpr int NW2 = (TT + SMAX + 1) / 2;
+#pragma unroll 1
+  for (int i = 0; i < n; ++i) {
+    const unsigned* src = reinterpret_cast<const unsigned*>(tile + slot[i] + lane_off);
+    unsigned w[NW2];
+#pragma unroll
+    for (int k = 0; k < NW2; ++k) w[k] = src[k];
+    unsigned short h[2 * NW2];
+    split_halves<NW2>(w, h);
+    const unsigned sh = pk[i];
+#pragma unroll
+    for (int j = 0; j < D; ++j) {
+      switch ((int)((sh >> (8 * j)) & 0xFFu)) {
+#define VFRB_G(S)                                                          \
+  case S:                                                                  \
+    if constexpr (S <= SMAX) pat_add_one_pair<TT, 2 * NW2, S>(acc[j], h);  \
+    break;
+        VFRB_CASES_0_31(VFRB_G)
+#undef VFRB_G
+        default:
+          break;
+      }
+    }
+  }
+}
+
 template <typename T, int TT, int NW, int S>
 __device__ __forceinline__ void pat_add_one(float (&acc)[TT], const typename PatElem<T>::R (&w)[NW]) {
 #pragma unroll
@@ -156,10 +234,24 @@ __device__ __forceinline__ void pat_run_generic(float (&acc)[D][TT], const T* ti
   }
 }
 
-template <typename T, int D, int TT, int SMAX>
+template <typename T, int D, int TT, int SMAX, bool PAIR = false>
 __device__ __forceinline__ void pat_dispatch(float (&acc)[D][TT], int pat, const T* tile, const int* slot,
                                              const unsigned* pk, int n, int lane_off) {
-  if constexpr (D == 4) {
+  if constexpr (PAIR) {
+    static_assert(sizeof(T) == 2 && D == 4, "pair form: FP16, four trials");
+    switch (pat) {
+#define VFRB_P4(ID, A, B, C)                                                                  \
+  case ID:                                                                                    \
+    if constexpr (PatMax<A, B, C>::v <= SMAX) pat_run_pair<D, TT, 0, A, B, C>(acc, tile, slot, n, lane_off); \
+    return;
+      VFRB_PAT4_LIST(VFRB_P4)
+#undef VFRB_P4
+      default:
+        break;
+    }
+    pat_run_generic_pair<D, TT, SMAX>(acc, tile, slot, pk, n, lane_off);
+    return;
+  } else if constexpr (D == 4) {
     switch (pat) {
 #define VFRB_P4(ID, A, B, C)                                                           \
   case ID:                                                                             \
@@ -221,12 +313,14 @@ __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, unsigned by
 }
 
 // W warps per CTA: 8 (two CTAs per SM, ~110 KB of tiles each) or 16 (one
-// CTA per SM sharing ~220 KB of tiles between twice as many DM trials)
-template <typename T, int D, int TT, int SMAX, int W>
+// CTA per SM sharing ~220 KB of tiles between twice as many DM trials).
+// PAIR: the FP16 pair form (two staged copies of each row, 4-byte loads).
+template <typename T, int D, int TT, int SMAX, int W, bool PAIR = false>
 __global__ void __launch_bounds__(W * 32, 16 / W) k_dedisp_pat(const DdPatParams pp) {
   // a batched launch: this CTA's stream's fields from its job
   DdPatParams p;
   p.fb = pp.fb;
+  p.fb1 = pp.fb1;
   p.out_scale = pp.out_scale;
   p.row0 = pp.row0;
   p.nrows_valid = pp.nrows_valid;
@@ -238,6 +332,7 @@ __global__ void __launch_bounds__(W * 32, 16 / W) k_dedisp_pat(const DdPatParams
   if (pp.njobs > 0) {
     const DdJob& j = pp.jobs[blockIdx.z];
     p.fb = j.fb;
+    p.fb1 = j.fb1;
     p.out_scale = j.out_scale;
     p.row0 = j.row0;
     p.nrows_valid = j.nrows_valid;
@@ -261,11 +356,13 @@ __global__ void __launch_bounds__(W * 32, 16 / W) k_dedisp_pat(const DdPatParams
   constexpr int VEC = 16 / (int)sizeof(T);
   constexpr int NT = 32 * TT;
   static_assert(sizeof(T) == 4 ? (TT & 1) == 1 : (TT & 3) == 2, "lane stride must spread loads over all banks");
+  static_assert(!PAIR || (sizeof(T) == 2 && D == 4), "pair form: FP16, four trials");
+  constexpr int NCOPY = PAIR ? 2 : 1;  // staged copies of each row: the row, and (PAIR) the row shifted by one
   extern __shared__ int4 smp4[];
   const int CH = p.chunk, LM = p.lmax;
   const int LMQ = LM / VEC;
   // shared layout: full[2] mbarriers (16 B) | slot[W][CH] int | pk[W][CH] unsigned | run[W][CH] int | nrun[W] int
-  //                | tiles[2][CH][LM] (16-byte aligned)
+  //                | tiles[2][NCOPY][CH][LM] (16-byte aligned)
   unsigned long long* s_full = reinterpret_cast<unsigned long long*>(smp4);
   int* s_slot = reinterpret_cast<int*>(smp4 + 1);
   unsigned* s_pk = reinterpret_cast<unsigned*>(s_slot + W * CH);
@@ -286,6 +383,7 @@ __global__ void __launch_bounds__(W * 32, 16 / W) k_dedisp_pat(const DdPatParams
   const long long t0 = (long long)tb * NT;
   const int g = min(blk * W + warp, p.ngroups - 1);
   const T* fb = reinterpret_cast<const T*>(p.fb);
+  const T* fb1 = reinterpret_cast<const T*>(p.fb1);  // PAIR: fb1[c][r] = fb[c][r + 1]
   const int nchunks = (p.nchan + CH - 1) / CH;
   const long long vend = p.row0 + p.nrows_valid;
   const unsigned long long rmask = (unsigned long long)p.row_mask;
@@ -333,39 +431,48 @@ __global__ void __launch_bounds__(W * 32, 16 / W) k_dedisp_pat(const DdPatParams
       const int cl = __ffs(slow) - 1;
       slow &= slow - 1;
       const long long ac = __shfl_sync(0xffffffffu, a, cl);
-      const T* src = fb + (long long)(c0 + cb + cl) * p.chan_stride;
-      int4* dst = tiles + ((long long)b * CH + cb + cl) * LMQ;
-      for (int v = lane; v < LMQ; v += 32) {
-        const long long r = ac + (long long)v * VEC;
-        int4 val = make_int4(0, 0, 0, 0);
-        if (r >= 0 && r + VEC <= vend) {  // a VEC-aligned group never straddles the ring end
-          val = *reinterpret_cast<const int4*>(src + ((unsigned long long)r & rmask));
-        } else if (r + VEC > 0 && r < vend) {
-          union {
-            int4 u;
-            T t[VEC];
-          } tmp;
-          tmp.u = make_int4(0, 0, 0, 0);
 #pragma unroll
-          for (int e = 0; e < VEC; ++e) {
-            const long long re = r + e;
-            if (re >= 0 && re < vend) tmp.t[e] = src[(unsigned long long)re & rmask];
+      for (int cp = 0; cp < NCOPY; ++cp) {
+        // copy cp holds rows r + cp of the filterbank (read as row r of fb1 for cp = 1)
+        const T* src = (cp ? fb1 : fb) + (long long)(c0 + cb + cl) * p.chan_stride;
+        int4* dst = tiles + (((long long)b * NCOPY + cp) * CH + cb + cl) * LMQ;
+        for (int v = lane; v < LMQ; v += 32) {
+          const long long r = ac + (long long)v * VEC;
+          int4 val = make_int4(0, 0, 0, 0);
+          if (r + cp >= 0 && r + VEC + cp <= vend) {  // a VEC-aligned group never straddles the ring end
+            val = *reinterpret_cast<const int4*>(src + ((unsigned long long)r & rmask));
+          } else if (r + VEC + cp > 0 && r + cp < vend) {
+            union {
+              int4 u;
+              T t[VEC];
+            } tmp;
+            tmp.u = make_int4(0, 0, 0, 0);
+#pragma unroll
+            for (int e = 0; e < VEC; ++e) {
+              const long long re = r + e;
+              if (re + cp >= 0 && re + cp < vend) tmp.t[e] = src[(unsigned long long)re & rmask];
+            }
+            val = tmp.u;
           }
-          val = tmp.u;
+          dst[v] = val;
         }
-        dst[v] = val;
       }
     }
     __syncwarp();
     const unsigned nbulk = __popc(__ballot_sync(0xffffffffu, bulk));
     fence_proxy_async_smem();  // earlier generic reads of this buffer before the async writes
-    if (lane == 0) mbar_arrive_expect_tx(&s_full[b], nbulk * (unsigned)(LM * (int)sizeof(T)));
+    if (lane == 0) mbar_arrive_expect_tx(&s_full[b], nbulk * (unsigned)(NCOPY * LM * (int)sizeof(T)));
     __syncwarp();
     if (bulk) {
-      int4* dst = tiles + ((long long)b * CH + cb + lane) * LMQ;
-      const T* src = fb + (long long)(c0 + cb + lane) * p.chan_stride;
-      bulk_g2s(dst, src + ra, (unsigned)(n1 * (int)sizeof(T)), &s_full[b]);
-      if (n1 < LM) bulk_g2s(dst + n1 / VEC, src, (unsigned)((LM - n1) * (int)sizeof(T)), &s_full[b]);
+      // the shifted copy's last element (row a + LM of the filterbank) may
+      // lie past the valid rows; no window reads it
+#pragma unroll
+      for (int cp = 0; cp < NCOPY; ++cp) {
+        int4* dst = tiles + (((long long)b * NCOPY + cp) * CH + cb + lane) * LMQ;
+        const T* src = (cp ? fb1 : fb) + (long long)(c0 + cb + lane) * p.chan_stride;
+        bulk_g2s(dst, src + ra, (unsigned)(n1 * (int)sizeof(T)), &s_full[b]);
+        if (n1 < LM) bulk_g2s(dst + n1 / VEC, src, (unsigned)((LM - n1) * (int)sizeof(T)), &s_full[b]);
+      }
     }
   };
 
@@ -402,6 +509,10 @@ __global__ void __launch_bounds__(W * 32, 16 / W) k_dedisp_pat(const DdPatParams
         rel = 0;
       }
       slot = lane * LM + rel;
+      if (PAIR) {  // the copy that puts the window's start (rel + lane * TT, TT even) on a 4-byte boundary
+        const int par = rel & 1;
+        slot += par * (CH * LM - 1);
+      }
       pk = m.pk;
       pat = m.pat;
     }
@@ -447,14 +558,14 @@ __global__ void __launch_bounds__(W * 32, 16 / W) k_dedisp_pat(const DdPatParams
     m_cur = meta_in(k + 1);
     if (!mbar_wait(&s_full[k & 1], (unsigned)(k >> 1) & 1u)) err |= kErrTimeout;
     const int b = k & 1;
-    const T* tile = reinterpret_cast<const T*>(tiles + (long long)b * CH * LMQ);
+    const T* tile = reinterpret_cast<const T*>(tiles + (long long)b * NCOPY * CH * LMQ);
     const int mb = warp * CH;
     const int nrun = s_nrun[warp];
 #pragma unroll 1
     for (int r = 0; r < nrun; ++r) {
       const int rd = s_run[mb + r];
       const int s0 = (rd >> 8) & 0xFF;
-      pat_dispatch<T, D, TT, SMAX>(acc, rd & 0xFF, tile, s_slot + mb + s0, s_pk + mb + s0, rd >> 16, lane * TT);
+      pat_dispatch<T, D, TT, SMAX, PAIR>(acc, rd & 0xFF, tile, s_slot + mb + s0, s_pk + mb + s0, rd >> 16, lane * TT);
     }
     __syncwarp();  // this warp's metadata is rewritten for the next chunk
   }

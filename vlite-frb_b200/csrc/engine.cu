@@ -229,6 +229,10 @@ struct StreamSt {
   cudaEvent_t ev_ready = nullptr;
   // both
   void* d_cm = nullptr;  // channel-major bandpassed FB (storage form)
+  // FP16 with dedispersion: the same ring shifted by one row,
+  // d_cm1[c][r] = d_cm[c][r + 1] (written by the bandpass beside d_cm), so
+  // the dedisperser reads its windows of halves with aligned 4-byte loads
+  void* d_cm1 = nullptr;
   int64_t cm_stride = 0;
   unsigned cm_mask = 0xffffffffu;
   float *d_w = nullptr, *d_inv = nullptr, *d_var = nullptr, *d_scr = nullptr;
@@ -334,6 +338,10 @@ size_t storage_bytes(int s) { return s == VFRB_F32 ? 4 : (s == VFRB_F16 ? 2 : 1)
 bool want(const vfrb_plan* pl, int bit) { return (pl->P.outputs & bit) != 0; }
 
 // device bytes one stream needs (admission control)
+// FP16 storage with dedispersion keeps the channel-major ring twice (the
+// second copy shifted by one row)
+bool shifted_copy(const vfrb_plan* pl) { return pl->P.storage == VFRB_F16 && pl->want_dd; }
+
 int64_t stream_bytes(const vfrb_plan* pl, int64_t ring_frames, int64_t R1, int64_t R2) {
   const vfrb_params& P = pl->P;
   const int64_t nch = pl->L.nchanout;
@@ -342,11 +350,11 @@ int64_t stream_bytes(const vfrb_plan* pl, int64_t ring_frames, int64_t R1, int64
   if (P.mode == VFRB_MODE_BLOCK) {
     b += (int64_t)pl->L.maxnt * nch * 4;                                    // raw block
     b += (int64_t)pl->max_delay * nch * 4;                                  // leftover
-    b += nch * (((int64_t)pl->L.maxnt + 15) / 16 * 16) * (int64_t)storage_bytes(P.storage);
+    b += nch * (((int64_t)pl->L.maxnt + 15) / 16 * 16) * (int64_t)storage_bytes(P.storage) * (shifted_copy(pl) ? 2 : 1);
     if (want(pl, VFRB_OUT_FB)) b += (int64_t)pl->L.maxnt * nch * 4;
     if (want(pl, VFRB_OUT_CHANSTATS)) b += 3LL * pl->nstatblks * nch * 4;
   } else {
-    b += R1 * nch * 4 + R2 * nch * (int64_t)storage_bytes(P.storage);
+    b += R1 * nch * 4 + R2 * nch * (int64_t)storage_bytes(P.storage) * (shifted_copy(pl) ? 2 : 1);
     if (want(pl, VFRB_OUT_CHANSTATS)) b += 4LL * nch * 4;
   }
   if (pl->want_dd) {
@@ -560,6 +568,7 @@ int run_bandpass(vfrb_plan* pl, StreamSt* s, const float* raw, int64_t in_row0, 
   a.tm_row_stride = pl->L.nchanout;
   a.d_err = s->d_err;
   a.subtract_mode = subtract_mode;
+  a.out_shift1 = pl->P.storage == VFRB_F16 ? s->d_cm1 : nullptr;
   return launch_bandpass(a, s->cs);
 }
 
@@ -591,6 +600,7 @@ int run_dedisp(vfrb_plan* pl, StreamSt* s, int64_t row0, int64_t nrows_valid, in
   a.frb = stats ? s->d_frb : nullptr;
   a.argmax = stats ? s->d_arg : nullptr;
   a.d_err = s->d_err;
+  a.fb_shift1 = pl->P.storage == VFRB_F16 ? s->d_cm1 : nullptr;
   ST(launch_dedisperse_plan(pl->dd, a, on ? on : s->cs));
   if (kernel_stats && boxcar_on(pl))
     ST(launch_boxcar(s->d_out, pl->ndm, nt, s->out_stride, s->d_ave, s->d_sgm, pl->P.boxcar_max, s->d_bsnr, s->d_bt,
@@ -831,6 +841,7 @@ int flush_batch(vfrb_plan* pl) {
     CK(cudaStreamWaitEvent(pl->bs, s->ev_ready, 0));
     DdJob j{};
     j.fb = s->d_cm;
+    j.fb1 = s->d_cm1;
     j.out_scale = pl->P.storage == VFRB_F16 ? s->uscale : 1.f;
     j.row0 = s->job_row0;
     j.nrows_valid = s->job_nvalid;
@@ -1152,6 +1163,10 @@ int create_stream(vfrb_plan* pl, int id, int64_t ring_frames, int64_t R1, int64_
     s->cm_stride = ((int64_t)L.maxnt + 15) / 16 * 16;
     s->cm_mask = 0xffffffffu;
     ST(dmalloc(s->res, &s->d_cm, (size_t)nch * s->cm_stride * sb));
+    if (shifted_copy(pl)) {
+      ST(dmalloc(s->res, &s->d_cm1, (size_t)nch * s->cm_stride * sb));
+      CK(cudaMemsetAsync(s->d_cm1, 0, (size_t)nch * s->cm_stride * sb, s->cs));
+    }
     if (want(pl, VFRB_OUT_FB)) ST(dmalloc(s->res, &s->d_fbt, (size_t)L.maxnt * nch * 4));
     if (want(pl, VFRB_OUT_CHANSTATS)) {
       ST(dmalloc(s->res, &s->d_cave, (size_t)pl->nstatblks * nch * 4));
@@ -1168,6 +1183,10 @@ int create_stream(vfrb_plan* pl, int id, int64_t ring_frames, int64_t R1, int64_
     s->cm_mask = (unsigned)(R2 - 1);
     ST(dmalloc(s->res, &s->d_cm, (size_t)nch * R2 * sb));
     CK(cudaMemsetAsync(s->d_cm, 0, (size_t)nch * R2 * sb, s->cs));
+    if (shifted_copy(pl)) {
+      ST(dmalloc(s->res, &s->d_cm1, (size_t)nch * R2 * sb));
+      CK(cudaMemsetAsync(s->d_cm1, 0, (size_t)nch * R2 * sb, s->cs));
+    }
     if (want(pl, VFRB_OUT_CHANSTATS)) {
       ST(dmalloc(s->res, &s->d_cave, (size_t)nch * 4));
       ST(dmalloc(s->res, &s->d_csig, (size_t)nch * 4));

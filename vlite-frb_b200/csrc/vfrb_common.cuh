@@ -30,6 +30,7 @@ inline int cuda_status(cudaError_t e) { return e == cudaSuccess ? VFRB_OK : VFRB
 // plan's.
 struct DdJob {
   const void* fb;
+  const void* fb1;  // FP16: the same ring shifted by one row (fb1[c][r] = fb[c][r + 1]), or NULL
   float out_scale;
   long long row0;
   long long nrows_valid;
