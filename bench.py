@@ -713,7 +713,7 @@ def main():
     f32 = run_device(vf, frames, 0, args.steps, args.warmup, dist, args.dd_variant)
     rtf = world * data_s / (f32["ms"] / 1000.0)
     # the FP16 form on the same resident data: the metric compares it with the FP32 form
-    f16 = run_device(vf, frames, 1, args.steps, args.warmup, dist)
+    f16 = run_device(vf, frames, 1, args.steps, args.warmup, dist, args.dd_variant)
     # e2e through the public plan API from page-locked host memory
     host = torch.empty(frames.numel(), dtype=torch.uint8, pin_memory=True)
     host.copy_(frames)
