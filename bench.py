@@ -814,9 +814,12 @@ def main():
         "gen_seconds": t_gen,
     }
     if f16 is not None:
+        k3_16 = units * nch / (f16["stage_ms"][2] / 1000.0)  # FP32 adds per second of the FP16 form's K3
         line["fp16"] = {"value": world * data_s / (f16["ms"] / 1000.0), "ms_per_step": f16["ms"],
                         "stages_ms_per_step": f16["stage_ms"], "speedup_vs_f32": f32["ms"] / f16["ms"],
                         "dedisperse_speedup_vs_f32": f32["stage_ms"][2] / f16["stage_ms"][2],
+                        "dedisperse_add_rate_tadd_s": k3_16 / 1e12,
+                        "dedisperse_fp32_add_peak_frac": k3_16 / fp32_peak_adds,
                         "autotune_ms": {"variant": f16["variant"], "times": {str(k): v for k, v in f16["tune"].items()}}}
         if e2e16_s is not None:  # through the plan API as well (PCIe-bound like the FP32 figure)
             line["fp16"]["e2e"] = {"value": world * data_s / e2e16_s, "unit": "s data/s",
