@@ -196,7 +196,9 @@ int vfrb_ddplan_variant(const vfrb_ddplan* plan, int storage);
 /* Times every applicable variant on scratch data of the given shape
  * (nt_out samples per trial, `storage` form) and keeps the fastest.  Writes
  * the per-variant times in ms to times[VFRB_DD_NVARIANTS] (index = variant,
- * < 0 = not applicable). */
+ * < 0 = not applicable).  FP16 variants are timed without a shifted ring
+ * (vfrb_dd_args.fb_shift1); given one, VFRB_DD_PAT4 runs its faster pair
+ * form, so the choice of PAT4 stands. */
 int vfrb_ddplan_autotune(vfrb_ddplan* plan, int storage, int64_t nt_out, float* times, void* stream);
 
 typedef struct vfrb_dd_args {
