@@ -43,11 +43,23 @@ __global__ void __launch_bounds__(kBpThreads) k_bandpass(const vfrb_bp_args a, _
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   int err = 0;
 
-  // load rows (time-major) -> tile[ch][row]
-  for (int r = warp; r < npts; r += kBpThreads / 32) {
-    const unsigned long long rr = (unsigned long long)(a.in_row0 + r0 + r) & (unsigned long long)a.in_row_mask;
+  // load rows (time-major) -> tile[ch][row]: a warp's 16 rows are loaded
+  // into registers first, so all 16 row segments are in flight together
+  {
+    constexpr int kRowsPerWarp = kBpMaxWin / (kBpThreads / 32);
+    float v[kRowsPerWarp];
     const int c = c0 + lane;
-    tile[lane][r] = (c < a.nchan) ? a.in[(long long)rr * a.in_row_stride + c] : 0.f;
+#pragma unroll
+    for (int k = 0; k < kRowsPerWarp; ++k) {
+      const int r = warp + (kBpThreads / 32) * k;
+      const unsigned long long rr = (unsigned long long)(a.in_row0 + r0 + r) & (unsigned long long)a.in_row_mask;
+      v[k] = (r < npts && c < a.nchan) ? a.in[(long long)rr * a.in_row_stride + c] : 0.f;
+    }
+#pragma unroll
+    for (int k = 0; k < kRowsPerWarp; ++k) {
+      const int r = warp + (kBpThreads / 32) * k;
+      if (r < npts) tile[lane][r] = v[k];
+    }
   }
   __syncthreads();
 
