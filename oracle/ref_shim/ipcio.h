@@ -13,6 +13,8 @@ typedef struct ipcio_t {
 } ipcio_t;
 /* the harness names the file that stands in for the shared-memory ring */
 void ref_shim_set_dada_file(const char* path);
+/* the iread value the next ipcio_connect finds (-1 unless set) */
+void ref_shim_set_iread(int iread);
 int ipcio_connect(ipcio_t* io, key_t key);
 int ipcio_open(ipcio_t* io, char rdwrt);
 long ipcio_read(ipcio_t* io, char* buf, size_t n);

@@ -1,12 +1,15 @@
 /* Project-written stand-ins for the libraries the reference links but this
  * repository cannot vendor: dedisp (always reports an error), a file-backed
  * psrdada reader, and getVDIFDMJD restated from the VDIF specification
- * (epoch = 6-month periods since 2000-01-01; seconds from the epoch start). */
+ * (epoch = 6-month periods since 2000-01-01; seconds from the epoch start).
+ * Built with REF_SHIM_DADA_ONLY, only the psrdada reader stand-in (the tests
+ * of the tools' psrdada input build it that way). */
 #include <stdio.h>
 #include <string.h>
 
-#include "dedisp.h"
 #include "ipcio.h"
+#ifndef REF_SHIM_DADA_ONLY
+#include "dedisp.h"
 #include "vdifio.h"
 
 dedisp_error dedisp_set_device(int device) { (void)device; return DEDISP_NO_ERROR; }
@@ -22,10 +25,14 @@ dedisp_error dedisp_execute(const dedisp_plan p, dedisp_size n, const dedisp_byt
   (void)p; (void)n; (void)i; (void)ib; (void)o; (void)ob; (void)f; return 1;
 }
 void dedisp_destroy_plan(dedisp_plan p) { (void)p; }
+#endif /* REF_SHIM_DADA_ONLY */
 
 static char g_dada_path[4096];
+static int g_iread = -1;
 void ref_shim_set_dada_file(const char* path) { strncpy(g_dada_path, path, sizeof(g_dada_path) - 1); }
-int ipcio_connect(ipcio_t* io, key_t key) { (void)key; memset(io, 0, sizeof(*io)); io->buf.iread = -1; return 0; }
+/* the iread value a connect finds (a stale primary reader when != -1) */
+void ref_shim_set_iread(int iread) { g_iread = iread; }
+int ipcio_connect(ipcio_t* io, key_t key) { (void)key; memset(io, 0, sizeof(*io)); io->buf.iread = g_iread; return 0; }
 int ipcio_open(ipcio_t* io, char rdwrt) {
   (void)rdwrt;
   io->buf.f = fopen(g_dada_path, "rb");
@@ -52,6 +59,7 @@ uint64_t ipcbuf_get_write_count(ipcbuf_t* b) { (void)b; return 0; }
 uint64_t ipcbuf_get_read_count(ipcbuf_t* b) { return b->nread; }
 int ipcbuf_get_nreaders(ipcbuf_t* b) { (void)b; return 1; }
 
+#ifndef REF_SHIM_DADA_ONLY
 /* days from 1970-01-01 of a Gregorian date */
 static long days_from_civil(long y, unsigned m, unsigned d) {
   y -= m <= 2;
@@ -68,3 +76,4 @@ int getVDIFFrameMJD(const vdif_header* h) {
 double getVDIFDMJD(const vdif_header* h, int fps) {
   return getVDIFFrameMJD(h) + (double)getVDIFFrameSecond(h) / 86400.0 + (double)getVDIFFrameNumber(h) / (fps * 86400.0);
 }
+#endif /* REF_SHIM_DADA_ONLY */

@@ -5,6 +5,11 @@
 
 Objects go to vlite-frb_b200/_build/, the library to vlite-frb_b200/lib/ and
 the tools to vlite-frb_b200/bin/.  Rebuilds only what changed.
+
+With PSRDADA_DIR set (a psrdada install: include/ipcio.h, lib/libpsrdada),
+the DADA tools (vdifDADA2stats, vdifDADA2timeseries) are built against
+psrdada and read the capture's own ring, as the reference tools do; without
+it they read the project's ring (vfrb_dada_*).
 """
 from __future__ import annotations
 
@@ -30,6 +35,18 @@ COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC,-Wall,-Wno-unus
 LIB_SOURCES = ["channelise.cu", "bandpass.cu", "rfi.cu", "dedisperse.cu", "vfrb_api.cpp"]
 LIB_SOURCES_OPTIONAL = ["engine.cu", "vdif_reader.cpp", "writers.cpp", "dada.cpp", "noalloc.cu", "candidates.cu", "cluster.cpp"]
 TOOL_MAINS = ["vdifFILE2dedisp_PIPELINE.cpp", "vdifDADA2stats.cpp", "vdifDADA2timeseries.cpp", "vfrb_dada_write.cpp"]
+DADA_TOOLS = ("vdifDADA2stats.cpp", "vdifDADA2timeseries.cpp")
+
+
+def psrdada_flags(main: str) -> list:
+    """Compile and link flags that put a DADA tool on psrdada's own ring
+    (PSRDADA_DIR set), else none."""
+    d = os.environ.get("PSRDADA_DIR")
+    if not d or main not in DADA_TOOLS:
+        return []
+    lib = os.path.join(d, "lib")
+    return ["-DVFRB_WITH_PSRDADA", "-I" + os.path.join(d, "include"), "-L" + lib, "-lpsrdada",
+            "-Xlinker", "-rpath," + lib]
 
 
 def _newer(src: str, dst: str, deps=()) -> bool:
@@ -90,7 +107,7 @@ def build(jobs: int = 8, verbose: bool = False) -> str:
             continue
         exe = os.path.join(BIN, m[:-4])
         if _newer(src, exe, headers + [so] + [os.path.join(TOOLS, h) for h in os.listdir(TOOLS) if h.endswith(".h")]):
-            _run([NVCC, *COMMON, "-x", "cu", src, "-o", exe, *ARCH, "-L" + LIB, "-lvfrb",
+            _run([NVCC, *COMMON, "-x", "cu", src, "-o", exe, *ARCH, *psrdada_flags(m), "-L" + LIB, "-lvfrb",
                   "-Xlinker", "-rpath," + LIB, "-Xlinker", "-rpath,$ORIGIN/../lib"])
     return "\n".join(logs)
 

@@ -16,6 +16,12 @@
 
 #include "vfrb.h"
 
+#ifdef VFRB_WITH_PSRDADA
+// psrdada's reader API (ipcio.h from psrdada; build.py adds it when
+// PSRDADA_DIR is set): the DADA tools then read the capture's own ring
+#include "ipcio.h"
+#endif
+
 namespace tool {
 
 inline bool eq(const char* a, const char* b) { return std::strcmp(a, b) == 0; }
@@ -47,7 +53,9 @@ inline bool file_exists(const char* p) { return access(p, F_OK) != -1; }
 inline bool write_all(FILE* f, const void* p, size_t n) { return n == 0 || std::fwrite(p, 1, n, f) == n; }
 
 // Byte source the tools read VDIF from: a file ("-" = standard input) or a
-// DADA-style ring named by its key (vfrb_dada_*).
+// ring named by its DADA key.  The ring is psrdada's own when the tools are
+// built with psrdada (VFRB_WITH_PSRDADA), otherwise the project's ring
+// (vfrb_dada_*, same reader-side behaviour).
 struct Source {
   FILE* f = nullptr;
   bool own = false;
@@ -64,11 +72,46 @@ struct Source {
     own = f != nullptr;
     return f != nullptr;
   }
+#ifdef VFRB_WITH_PSRDADA
+  ipcio_t dada{};  // zero-initialised, as the reference's global ipcio_t
+  bool psrdada = false;
+  // psrdada's ring: ipcio_connect, the iread force on the ipcbuf_t that the
+  // ipcio_t begins with (iread = -1 is required to open as the primary read
+  // client), ipcio_open('R') and the ring's counters in the log, as the
+  // reference does (STATS:123-134, 284-304; TS:136-147, 357-382).  Returns
+  // 0, 1 (could not connect) or 2 (could not open as the primary reader).
+  int connect_psrdada(uint32_t key, FILE* log) {
+    if (ipcio_connect(&dada, (key_t)key) < 0) return 1;
+    ipcbuf_t* b = reinterpret_cast<ipcbuf_t*>(&dada);
+    if (b->iread != -1) {
+      std::fprintf(log, " iread= %d != -1, setting to -1\n", b->iread);
+      b->iread = -1;
+    } else {
+      std::fprintf(log, " iread= %d, do not need to force\n", b->iread);
+    }
+    if (ipcio_open(&dada, 'R') < 0) {
+      ipcio_disconnect(&dada);
+      return 2;
+    }
+    psrdada = true;
+    std::fprintf(log, " nbufs= %lu\n", (unsigned long)ipcbuf_get_nbufs(b));
+    std::fprintf(log, " bufsz= %lu\n", (unsigned long)ipcbuf_get_bufsz(b));
+    std::fprintf(log, " nfull= %lu\n", (unsigned long)ipcbuf_get_nfull(b));
+    std::fprintf(log, " nclear= %lu\n", (unsigned long)ipcbuf_get_nclear(b));
+    std::fprintf(log, " write count= %lu\n", (unsigned long)ipcbuf_get_write_count(b));
+    std::fprintf(log, " read count = %lu\n", (unsigned long)ipcbuf_get_read_count(b));
+    return 0;
+  }
+#endif
   // ipcio_connect, then the reference's iread force and ipcio_open('R')
   // (STATS:284-298, TS:357-372) with its log lines; waits (bounded) for the
   // writer's ring.  Returns 0, 1 (could not connect) or 2 (could not open
   // as the primary reader).
   int connect(uint32_t key, FILE* log, int wait_ms = 30000) {
+#ifdef VFRB_WITH_PSRDADA
+    (void)wait_ms;
+    return connect_psrdada(key, log);
+#endif
     const double t0 = now_s();
     while (vfrb_dada_connect(key, &ring) != VFRB_OK) {
       if ((now_s() - t0) * 1e3 > wait_ms) return 1;
@@ -97,6 +140,17 @@ struct Source {
   }
   void release(size_t n) { vfrb_dada_release(ring, n); }
   size_t read(void* buf, size_t n) {
+#ifdef VFRB_WITH_PSRDADA
+    // a short read is the end of data (the reference then checks ipcbuf_eod)
+    if (psrdada) {
+      const long k = (long)ipcio_read(&dada, static_cast<char*>(buf), n);
+      if (k < 0) {
+        failed = true;
+        return 0;
+      }
+      return (size_t)k;
+    }
+#endif
     if (ring) {
       const int64_t k = vfrb_dada_read(ring, buf, n, timeout_ms);
       if (k < 0) {
@@ -110,6 +164,12 @@ struct Source {
   ~Source() {
     if (own) std::fclose(f);
     if (ring) vfrb_dada_close(ring);
+#ifdef VFRB_WITH_PSRDADA
+    if (psrdada) {
+      ipcio_close(&dada);
+      ipcio_disconnect(&dada);
+    }
+#endif
   }
 };
 
